@@ -1,0 +1,201 @@
+/*
+ * ds_api.h -- C ABI of the B200 dual simplex engine (libds_b200.so).
+ *
+ * The entry points replace the solver surface of veret-v/parallel_ds, which
+ * is C++ only (no C ABI).  Each declaration cites the reference interface it
+ * stands in for, by file:line within that project.
+ *
+ * Conventions
+ *   - Every function returns 0 (DS_OK) on success and a negative DS_ERR_* code
+ *     on failure; no C++ exception crosses this boundary.  ds_last_error()
+ *     returns a message for the last failure on a handle.
+ *   - Host pointers only; inputs are copied, the caller keeps ownership.
+ *   - A bound with |v| > 1e100 is infinite (reference problem.hpp:31,83).
+ *   - Variables are numbered like the reference's computational form
+ *     (problem.tpp:176-226): columns 0..n-1 are the structurals, n..n+m-1 the
+ *     row slacks, with A x + s = 0 and s in [-row_ub, -row_lb].
+ *   - One handle per host thread; each handle owns a CUDA stream.
+ */
+#ifndef DS_API_H
+#define DS_API_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ------------------------------------------------------- */
+#define DS_OK               0
+#define DS_ERR_ARG         -1   /* bad argument (null pointer, bad size)      */
+#define DS_ERR_CUDA        -2   /* CUDA runtime failure                       */
+#define DS_ERR_STATE       -3   /* call out of order (e.g. solve before load) */
+#define DS_ERR_SHAPE       -4   /* m > n: reference problem.tpp:230-239       */
+#define DS_ERR_NUMERIC     -5   /* singular basis / NaN in the iteration      */
+#define DS_ERR_DEVICE_WAIT -6   /* a bounded device-side wait ran out         */
+#define DS_ERR_CAPACITY    -7   /* a size exceeds a fixed capacity            */
+
+/* ---- solution status (reference LPsolution.message values) ------------- */
+#define DS_STATUS_UNSOLVED          0
+#define DS_STATUS_OPTIMAL           1  /* "optimal solution" cudaDualSimplex.cpp:451 */
+#define DS_STATUS_PRIMAL_INFEASIBLE 2  /* "dual unbounded"   cudaDualSimplex.cpp:500 */
+#define DS_STATUS_DUAL_INFEASIBLE   3  /* "dual infeasible"  baseDualSimplex.tpp:851 */
+#define DS_STATUS_ITER_LIMIT        4  /* reference has no limit (MAX_ITER unused)   */
+#define DS_STATUS_ERROR             5
+
+/* ---- bound types: same order as reference enum BoundaryType (types.hpp:49-57) */
+#define DS_FIXED 0
+#define DS_FREE  1
+#define DS_BOXED 2
+#define DS_UPPER 3   /* only an upper bound */
+#define DS_LOWER 4   /* only a lower bound  */
+
+/* ---- pricing rules ------------------------------------------------------ */
+#define DS_PRICING_DSE     0   /* dual steepest edge, baseDualSimplex.tpp:470-501  */
+#define DS_PRICING_LEARNED 1   /* MLP leaving-row scorer with DSE fallback (new)   */
+
+typedef struct ds_options {
+    int    refactor_interval;  /* REFACT_FREQ (baseDualSimplex.hpp:41 = 150); default 100 */
+    int    max_iterations;     /* iteration cap -> DS_STATUS_ITER_LIMIT; default 2,000,000 */
+    int    pricing;            /* DS_PRICING_*                                     */
+    int    strict_reference;   /* 1: reproduce the reference's control flow with no
+                                  engine guards (no post-perturbation cleanup, no
+                                  restart-loop guard)                               */
+    unsigned long long seed;   /* seeds the cost perturbation (the reference draws
+                                  from std::random_device, baseDualSimplex.tpp:244) */
+    int    device;             /* CUDA device ordinal                              */
+    void*  stream;             /* cudaStream_t to use, or NULL for an own stream   */
+    double learned_margin;     /* learned pricing: minimum score margin over the
+                                  runner-up before the network's row is taken      */
+    int    verbose;            /* 0 silent, 1 events, 2 every iteration            */
+} ds_options;
+
+typedef struct ds_stats {
+    int    iterations;         /* reference `iteration` counter (phase 1 + 2)      */
+    int    phase1_iterations;
+    int    refactors;
+    int    restarts;
+    int    perturbed;
+    int    bfrt_flips;
+    int    learned_used;       /* iterations where the network's row was taken     */
+    int    learned_fallback;   /* iterations that fell back to DSE                 */
+    int    bump_size;          /* structurals in the last factorised basis         */
+    int    kernel_launches;    /* kernels launched by the solve                    */
+    double solve_ms;           /* device time of ds_solve (CUDA events)            */
+    double refactor_ms;        /* device time spent refactorising                  */
+} ds_stats;
+
+typedef struct ds_solver ds_solver;
+
+void        ds_default_options(ds_options* opts);
+const char* ds_version(void);
+
+/* Create/destroy a solver handle.
+ * Replaces CudaDualSimplex(problem) + initDualSimplex()
+ * (cudaDualSimplex.hpp:83-86, cudaDualSimplex.cpp:20-81). */
+int ds_create(const ds_options* opts, ds_solver** out);
+int ds_destroy(ds_solver* s);
+
+/* Load min c^T x, row_lb <= A x <= row_ub, col_lb <= x <= col_ub with A in CSR.
+ * Bound types follow Problem::readMps (problem.tpp:350-395); slacks follow
+ * transformToComputeForm (problem.tpp:176-226). */
+int ds_load_csr(ds_solver* s, int m, int n,
+                const int* row_ptr, const int* col_idx, const double* val,
+                const double* c,
+                const double* col_lb, const double* col_ub,
+                const double* row_lb, const double* row_ub);
+
+/* Load with explicit bound types: the reference's 8-argument Problem ctor
+ * (problem.tpp:143-173) -- bound_type, range_type, costs, lower_range,
+ * upper_range, lower_bound, upper_bound, A(CSR, matrix.cpp:21-36). */
+int ds_load_typed(ds_solver* s, int m, int n,
+                  const int* row_ptr, const int* col_idx, const double* val,
+                  const double* c,
+                  const int* col_type, const double* col_lb, const double* col_ub,
+                  const int* row_type, const double* row_lb, const double* row_ub);
+
+/* presolve("minInfeas") + solve() + postProcess
+ * (baseDualSimplex.tpp:5-30, 164-180, 123-159; main.cpp:84-87). */
+int ds_solve(ds_solver* s);
+
+int    ds_get_status(const ds_solver* s);
+/* c^T x of the final point (recomputed, not the incremental value). */
+double ds_get_objective(const ds_solver* s);
+/* Problem::getSolution x (problem.tpp:243-259): x[n] structurals, slacks[m] (may be NULL). */
+int    ds_get_primal(const ds_solver* s, double* x, double* slacks);
+/* Row duals y_i = -d_{n+i}; the reference keeps d protected (baseDualSimplex.hpp:76). */
+int    ds_get_dual(const ds_solver* s, double* y);
+int    ds_get_reduced_costs(const ds_solver* s, double* d);
+int    ds_get_iterations(const ds_solver* s);
+int    ds_get_stats(const ds_solver* s, ds_stats* st);
+/* Basis as variable indices per basis position (basis_indexes, baseDualSimplex.hpp:80). */
+int    ds_get_basis(const ds_solver* s, int* basis);
+const char* ds_last_error(const ds_solver* s);
+
+/* Record (p, q, theta, objective) per phase-2 iteration into caller arrays
+ * (the reference prints these lines under DEBUG, cudaDualSimplex.cpp:636-641).
+ * Pass cap = 0 to stop tracing. */
+int ds_set_trace(ds_solver* s, int cap);
+int ds_get_trace(const ds_solver* s, int* p, int* q, double* theta, double* obj, int* count);
+
+
+/* ---- kernel-level entry points (run one device kernel on host vectors) ----
+ * For index-selection parity against the reference on identical inputs. */
+
+/* CHUZR: BaseDualSimplex::DSEPricing + checkVarIsInfeas (baseDualSimplex.tpp:443-501)
+ * with an empty blocked set; also returns checkPrimalFeasible (tpp:296-324). */
+int ds_kernel_dse_pricing(int m, int N, const int* basis, const double* x,
+                          const double* lb, const double* ub, const int* type,
+                          const double* beta,
+                          int* p, int* p_idx, double* delta, int* is_lower,
+                          int* primal_feasible);
+
+/* Pivot row: CudaSparseMatrix::dotUpdate(UPDATE_T) for alpha=1, beta=0
+ * (cudaSparseMatrix.cpp:359-378; CPU order matrix.cpp:273-286).
+ * A is the structural CSC (n columns); slack columns are implicit. */
+int ds_kernel_pivot_row(int m, int n, const int* csc_ptr, const int* csc_row,
+                        const double* csc_val, const int* nonbasis,
+                        const double* rho, double* alpha);
+
+/* CHUZC: simpleRatioTestPart1 + simpleRatioTest + the bound-flipping loop
+ * (cudaDualSimplex.cpp:367-394, 484-549; baseDualSimplex.tpp:546-572).
+ * alpha is the un-negated pivot row; delta the signed primal infeasibility. */
+int ds_kernel_ratio_test(int n, int N, const int* nonbasis, const double* alpha,
+                         double delta, int is_lower,
+                         const double* x, const double* d,
+                         const double* lb, const double* ub, const int* type,
+                         int* q, int* q_idx, double* theta, double* delta_out,
+                         int* num_candidates);
+
+/* PFI eta file: linalg::PFIsolve (linalg.cpp:12-46) / etaSolveKernel
+ * (cudaKernels.cu:266-322): apply T eta columns (eta[t*m + i], pivots pos[t])
+ * forward (transpose=0) or backward (transpose=1) to rhs, result in sol. */
+int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos,
+                        const double* rhs, double* sol, int transpose);
+
+/* ---- seeded LP generator (shared by tests, bench and the trainer) ---------- */
+#define DS_GEN_DENSITY   0   /* Bernoulli(density) per entry                   */
+#define DS_GEN_PER_COL   1   /* exactly per_col nonzeros per column            */
+#define DS_GEN_BLOCK     2   /* block-angular: blocks + linking rows           */
+typedef struct ds_gen_spec {
+    int kind;
+    int m, n;
+    double density;
+    int per_col;
+    int blocks, block_m, block_n, link_rows;
+    double block_density, link_density;
+    unsigned long long seed;
+} ds_gen_spec;
+/* Writes A (CSR), b (m) and c (n) of min c^T x, A x <= b, x >= 0 with
+ * A ~ N(0,1) entries, x0 ~ U[0,1], b = A x0 + U[0.1,1], c ~ U[0,1].
+ * Returns nnz; when val is NULL or capacity < nnz only counts. */
+long long ds_gen_lp(const ds_gen_spec* spec, int* row_ptr, int* col_idx, double* val,
+                    double* b, double* c, long long capacity);
+/* Row count m of batched instance i (m ~ U{m_lo..m_hi}, seeded by seed+i). */
+int ds_gen_batch_m(unsigned long long seed, int i, int m_lo, int m_hi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DS_API_H */

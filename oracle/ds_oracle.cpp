@@ -1,0 +1,899 @@
+// TEST INFRASTRUCTURE ONLY -- CPU restatement of veret-v/parallel_ds's
+// sequential bounded dual simplex (parity checker for the CUDA engine).
+//
+// Every routine names the reference lines it restates.  Paths are relative to
+// the reference project root.  Arithmetic is written in the reference's
+// operation order and built with -ffp-contract=off so that single operations
+// round exactly as the reference's unfused x86-64 code does.
+//
+// Departures, each guarded by or_options and documented in DESIGN.md:
+//   * PARDISO (src/cpu/matrix.cpp:530-583) is replaced by a dense LU with
+//     partial pivoting of the basis's structural block K = A[R', S]; slack
+//     columns of the basis are eliminated exactly (they are unit columns).
+//   * std::random_device in perturbCosts (baseDualSimplex.tpp:244) becomes a
+//     seeded std::mt19937 so runs are repeatable.
+//   * strict_reference = 0 adds two guards: a restart-loop stop and a
+//     post-perturbation cleanup (phase 1 + phase 2 on the original costs when
+//     the perturbed optimum is dual infeasible; the reference's callPrimalSolver
+//     is an empty stub, baseDualSimplex.tpp:677-680).
+#include "ds_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <unordered_set>
+#include <vector>
+
+namespace {
+
+// Tolerances and constants: baseDualSimplex.hpp:23-46.
+constexpr double EPS_BOUND = 1e-10;
+constexpr double EPS_D = 1e-7;
+constexpr double EPS_COSTS = 1e-8;
+constexpr double EPS_A = 1e-5;
+constexpr double EPS_Z = 1e-10;
+constexpr double EPS_R = 1e-9;
+constexpr double EPS_F = 1e-10;
+constexpr double PERTURB_RATIO = 0.25;
+constexpr double PSI = 1e-5;
+constexpr int MAX_CYCLE = 5;
+constexpr int NEED_RESTART = 40;
+constexpr double INF = 1e25;
+constexpr double BOUND_INF = 1e100;  // problem.hpp:31
+
+enum { FIXED = 0, FREE = 1, BOXED = 2, UPPER = 3, LOWER = 4 };
+enum { ST_UNSOLVED = 0, ST_OPTIMAL = 1, ST_PRIMAL_INF = 2, ST_DUAL_INF = 3, ST_ITER = 4, ST_ERROR = 5 };
+enum Phase1Out { P1_SOLVED, P1_DUALINF, P1_RESTART };
+
+struct Stop {};  // thrown to unwind on iteration limit / numeric failure
+
+struct Oracle {
+    or_options opt{};
+    int m = 0, n = 0, N = 0;
+    // [A | I] in CSC (rows ascending) and CSR (slack entry last in each row):
+    // Matrix::genSparseReprs (matrix.cpp:99-146), stackColUnitMatrix (matrix.cpp:349-372).
+    std::vector<int> cptr, crow, rptr, rcol;
+    std::vector<double> cval, rval;
+    std::vector<double> lb, ub, costs, original_costs, diff_bounds;
+    std::vector<int> type;
+
+    std::vector<double> x, d, beta;
+    std::vector<int> basis, nonbasis;
+    std::vector<char> is_basic;
+
+    // factor of B0: K = A[rp_row, s_var], P K = L U
+    int k = 0;
+    std::vector<int> s_pos, s_var, rp_row, row_slackpos, piv;
+    std::vector<double> LU;
+    // PFI eta file (PFIfactor / linalg::PFIsolve)
+    std::vector<std::vector<double>> eta;
+    std::vector<int> eta_p;
+
+    int iteration = 0, phase1_iters = 0, refactors = 0, restarts = 0, flips = 0;
+    long long pivots = 0;  // basis changes in either phase
+    bool perturbed = false;
+    double obj = 0.0;
+    int status = ST_UNSOLVED;
+    std::mt19937 gen;
+    bool in_phase1 = false;
+
+    // trace
+    int* tp = nullptr; int* tq = nullptr; double* tth = nullptr; double* tob = nullptr;
+    int tcap = 0, tcount = 0;
+
+    // ---------------------------------------------------------------- setup
+    void load(int m_, int n_, const int* row_ptr, const int* col_idx, const double* val,
+              const double* c, const int* col_type, const double* col_lb, const double* col_ub,
+              const int* row_type, const double* row_lb, const double* row_ub) {
+        m = m_; n = n_; N = n + m;
+        // CSR of [A | I]
+        rptr.assign(m + 1, 0);
+        for (int i = 0; i < m; ++i) rptr[i + 1] = rptr[i] + (row_ptr[i + 1] - row_ptr[i]) + 1;
+        rcol.resize(rptr[m]); rval.resize(rptr[m]);
+        for (int i = 0; i < m; ++i) {
+            int p = rptr[i];
+            for (int e = row_ptr[i]; e < row_ptr[i + 1]; ++e) { rcol[p] = col_idx[e]; rval[p] = val[e]; ++p; }
+            rcol[p] = n + i; rval[p] = 1.0;
+        }
+        // CSC by walking rows in order
+        cptr.assign(N + 1, 0);
+        for (int e = 0; e < rptr[m]; ++e) cptr[rcol[e] + 1]++;
+        for (int j = 0; j < N; ++j) cptr[j + 1] += cptr[j];
+        crow.resize(rptr[m]); cval.resize(rptr[m]);
+        std::vector<int> cur(cptr.begin(), cptr.end() - 1);
+        for (int i = 0; i < m; ++i)
+            for (int e = rptr[i]; e < rptr[i + 1]; ++e) { int p = cur[rcol[e]]++; crow[p] = i; cval[p] = rval[e]; }
+        // bounds / types: structurals as given, slacks per transformToComputeForm
+        lb.resize(N); ub.resize(N); costs.resize(N); type.resize(N);
+        for (int j = 0; j < n; ++j) { lb[j] = col_lb[j]; ub[j] = col_ub[j]; costs[j] = c[j]; type[j] = col_type[j]; }
+        for (int i = 0; i < m; ++i) {
+            ub[n + i] = -row_lb[i];
+            lb[n + i] = -row_ub[i];
+            costs[n + i] = 0;
+            switch (row_type[i]) {
+                case FIXED: type[n + i] = FIXED; break;
+                case BOXED: type[n + i] = BOXED; break;
+                case LOWER: type[n + i] = UPPER; break;
+                case UPPER: type[n + i] = LOWER; break;
+                default: type[n + i] = FREE; break;  // reference has no case (problem.tpp:201-218)
+            }
+        }
+        diff_bounds.resize(N);
+        for (int j = 0; j < N; ++j) diff_bounds[j] = ub[j] - lb[j];
+        // BaseDualSimplex ctor (baseDualSimplex.tpp:184-204): slack basis
+        basis.resize(m); nonbasis.resize(n); is_basic.assign(N, 0);
+        for (int i = 0; i < n; ++i) nonbasis[i] = i;
+        for (int i = 0; i < m; ++i) { basis[i] = i + n; is_basic[i + n] = 1; }
+        beta.assign(m, 0.0);
+        x.assign(N, 0.0); d.assign(N, 0.0);
+        gen.seed((unsigned)(opt.seed & 0xffffffffu) ^ (unsigned)(opt.seed >> 32));
+    }
+
+    void tick() {
+        if (iteration > opt.max_iterations) { status = ST_ITER; throw Stop{}; }
+    }
+
+    // ---------------------------------------------------------------- factor
+    // reFactorize (sequentialDualSimplex.cpp:155-160): clear eta file, B <- A[:,basis], LU.
+    void refactor() {
+        ++refactors;
+        eta.clear(); eta_p.clear();
+        s_pos.clear(); s_var.clear(); rp_row.clear();
+        row_slackpos.assign(m, -1);
+        for (int i = 0; i < m; ++i) {
+            int v = basis[i];
+            if (v < n) { s_pos.push_back(i); s_var.push_back(v); }
+            else row_slackpos[v - n] = i;
+        }
+        for (int r = 0; r < m; ++r) if (row_slackpos[r] < 0) rp_row.push_back(r);
+        k = (int)s_pos.size();
+        if ((int)rp_row.size() != k) { status = ST_ERROR; throw Stop{}; }
+        std::vector<int> rowk(m, -1);
+        for (int t = 0; t < k; ++t) rowk[rp_row[t]] = t;
+        LU.assign((size_t)k * k, 0.0);  // row-major K[t][j]
+        for (int j = 0; j < k; ++j)
+            for (int e = cptr[s_var[j]]; e < cptr[s_var[j] + 1]; ++e) {
+                int t = rowk[crow[e]];
+                if (t >= 0) LU[(size_t)t * k + j] = cval[e];
+            }
+        piv.resize(k);
+        for (int c = 0; c < k; ++c) {
+            int pr = c; double best = std::fabs(LU[(size_t)c * k + c]);
+            for (int r = c + 1; r < k; ++r) { double v = std::fabs(LU[(size_t)r * k + c]); if (v > best) { best = v; pr = r; } }
+            piv[c] = pr;
+            if (!(best > 1e-14)) { status = ST_ERROR; throw Stop{}; }
+            if (pr != c) for (int j = 0; j < k; ++j) std::swap(LU[(size_t)c * k + j], LU[(size_t)pr * k + j]);
+            const double pv = LU[(size_t)c * k + c];
+            double* rowc = &LU[(size_t)c * k];
+
+            for (int r = c + 1; r < k; ++r) {
+                double* rowr = &LU[(size_t)r * k];
+                const double l = rowr[c] / pv;
+                rowr[c] = l;
+                if (l != 0.0)
+                    for (int j = c + 1; j < k; ++j) rowr[j] -= l * rowc[j];
+            }
+        }
+    }
+    // K z = b (b, z length k), PK = LU
+    void k_solve(std::vector<double>& z) const {
+        for (int c = 0; c < k; ++c) if (piv[c] != c) std::swap(z[c], z[piv[c]]);
+        for (int r = 0; r < k; ++r) { double s = z[r]; const double* row = &LU[(size_t)r * k]; for (int j = 0; j < r; ++j) s -= row[j] * z[j]; z[r] = s; }
+        for (int r = k - 1; r >= 0; --r) { double s = z[r]; const double* row = &LU[(size_t)r * k]; for (int j = r + 1; j < k; ++j) s -= row[j] * z[j]; z[r] = s / row[r]; }
+    }
+    // K^T z = b: U^T w = b, L^T v = w, z = P^T v
+    void kt_solve(std::vector<double>& z) const {
+        // row sweeps: U^T w = b, then L^T v = w (unit diagonal), then undo P
+        for (int j = 0; j < k; ++j) {
+            const double* row = &LU[(size_t)j * k];
+            const double wj = z[j] / row[j];
+            z[j] = wj;
+            if (wj != 0.0) for (int r = j + 1; r < k; ++r) z[r] -= row[r] * wj;
+        }
+        for (int j = k - 1; j >= 0; --j) {
+            const double* row = &LU[(size_t)j * k];
+            const double vj = z[j];
+            if (vj != 0.0) for (int r = 0; r < j; ++r) z[r] -= row[r] * vj;
+        }
+        for (int c = k - 1; c >= 0; --c) if (piv[c] != c) std::swap(z[c], z[piv[c]]);
+    }
+    // B0 x = b (b by rows, x by positions): Matrix::solve non-transposed.
+    void b0_solve(const std::vector<double>& b, std::vector<double>& out) const {
+        std::vector<double> z(k);
+        for (int t = 0; t < k; ++t) z[t] = b[rp_row[t]];
+        k_solve(z);
+        out.assign(m, 0.0);
+        std::vector<double> xs_of_var;  // dense lookup of structural solution by column
+        std::vector<int> kcol(n, -1);
+        for (int j = 0; j < k; ++j) { out[s_pos[j]] = z[j]; kcol[s_var[j]] = j; }
+        for (int r = 0; r < m; ++r) {
+            int i = row_slackpos[r];
+            if (i < 0) continue;
+            double s = b[r];
+            for (int e = rptr[r]; e < rptr[r + 1]; ++e) {
+                int c = rcol[e];
+                if (c < n && kcol[c] >= 0) s -= rval[e] * z[kcol[c]];
+            }
+            out[i] = s;
+        }
+    }
+    // B0^T y = c (c by positions, y by rows): Matrix::solve transposed.
+    void b0t_solve(const std::vector<double>& c, std::vector<double>& y) const {
+        y.assign(m, 0.0);
+        std::vector<char> inR(m, 0);
+        for (int r = 0; r < m; ++r) if (row_slackpos[r] >= 0) { y[r] = c[row_slackpos[r]]; inR[r] = 1; }
+        std::vector<double> z(k);
+        for (int j = 0; j < k; ++j) {
+            double s = c[s_pos[j]];
+            for (int e = cptr[s_var[j]]; e < cptr[s_var[j] + 1]; ++e)
+                if (inR[crow[e]]) s -= cval[e] * y[crow[e]];
+            z[j] = s;
+        }
+        kt_solve(z);
+        for (int t = 0; t < k; ++t) y[rp_row[t]] = z[t];
+    }
+    // linalg::PFIsolve (linalg.cpp:12-46)
+    void pfi(std::vector<double>& sol, bool transpose) const {
+        const int T = (int)eta.size();
+        if (!transpose) {
+            for (int t = 0; t < T; ++t) {
+                const int kk = eta_p[t]; const double* ev = eta[t].data();
+                const double sk = sol[kk];
+                for (int i = 0; i < m; ++i) sol[i] = sol[i] + sk * ev[i];
+                sol[kk] = sk * ev[kk];
+            }
+        } else {
+            for (int t = T - 1; t >= 0; --t) {
+                const int kk = eta_p[t]; const double* ev = eta[t].data();
+                double s = 0.0;
+                for (int i = 0; i < m; ++i) s += ev[i] * sol[i];
+                sol[kk] = s;
+            }
+        }
+    }
+    // SequentialDualSimplex::solveLinSys (sequentialDualSimplex.cpp:28-70)
+    void ftran(const std::vector<double>& rhs, std::vector<double>& sol) const { b0_solve(rhs, sol); pfi(sol, false); }
+    void btran(const std::vector<double>& rhs, std::vector<double>& sol) const {
+        std::vector<double> tmp = rhs; pfi(tmp, true); b0t_solve(tmp, sol);
+    }
+
+    // ---------------------------------------------------------------- helpers
+    // checkVarIsInfeas (baseDualSimplex.tpp:443-466), switch fallthrough kept.
+    std::pair<bool, double> var_infeas(int i) const {
+        switch (type[i]) {
+            case LOWER:
+                if (x[i] < lb[i] - EPS_BOUND) return {true, x[i] - lb[i]};
+                [[fallthrough]];
+            case UPPER:
+                if (x[i] > ub[i] + EPS_BOUND) return {true, x[i] - ub[i]};
+                [[fallthrough]];
+            case FIXED:
+                if (std::fabs(x[i] - lb[i]) < EPS_BOUND) return {true, x[i] - lb[i]};
+                [[fallthrough]];
+            case BOXED:
+                if (x[i] > ub[i] + EPS_BOUND) return {true, x[i] - ub[i]};
+                else if (x[i] < lb[i] - EPS_BOUND) return {true, x[i] - lb[i]};
+        }
+        return {false, 0.0};
+    }
+    // checkPrimalFeasible (tpp:296-324), fallthrough kept.
+    bool primal_feasible() const {
+        for (int i : basis) {
+            switch (type[i]) {
+                case FIXED:
+                    if (std::fabs(x[i] - lb[i]) > EPS_BOUND) return false;
+                    [[fallthrough]];
+                case FREE: break;
+                case BOXED:
+                    if (x[i] > ub[i] + EPS_R * std::fabs(ub[i]) + EPS_BOUND || x[i] < lb[i] - EPS_R * std::fabs(lb[i]) - EPS_BOUND) return false;
+                    [[fallthrough]];
+                case UPPER:
+                    if (x[i] > ub[i] + EPS_R * std::fabs(ub[i]) + EPS_BOUND) return false;
+                    [[fallthrough]];
+                case LOWER:
+                    if (x[i] < lb[i] - EPS_R * std::fabs(lb[i]) - EPS_BOUND) return false;
+            }
+        }
+        return true;
+    }
+    // checkDualFeasible / counterDualInfeasible (tpp:362-440)
+    int dual_infeasible_count() const {
+        int num = 0;
+        for (int i : nonbasis) {
+            switch (type[i]) {
+                case FREE: if (std::fabs(d[i]) < EPS_D || std::isnan(d[i])) num++; break;
+                case UPPER: if (d[i] > EPS_D || std::isnan(d[i])) num++; break;
+                case LOWER: if (d[i] < -EPS_D || std::isnan(d[i])) num++; break;
+                default: break;
+            }
+        }
+        return num;
+    }
+    bool dual_feasible() const { return dual_infeasible_count() == 0; }
+
+    // setPrimalVars (tpp:74-101)
+    void set_primal_vars() {
+        for (int i : nonbasis) {
+            switch (type[i]) {
+                case FIXED: x[i] = lb[i]; break;
+                case FREE: x[i] = 0; break;
+                case BOXED: x[i] = (d[i] > 0) ? lb[i] : ub[i]; break;
+                case UPPER: x[i] = ub[i]; break;
+                case LOWER: x[i] = lb[i]; break;
+            }
+        }
+    }
+    // initBetaWeights (tpp:34-70)
+    void init_beta(bool ibasis) {
+        if (ibasis) { for (int i = 0; i < m; ++i) beta[i] = 1; return; }
+        std::vector<double> e(m, 0.0), buf;
+        for (int i = 0; i < m; ++i) {
+            e.assign(m, 0.0); e[i] = 1;
+            btran(e, buf);
+            double s = 0; for (double v : buf) s += v * v;  // ValuesVector::norm = sum of squares
+            beta[i] = s;
+        }
+    }
+    // initReducedCosts (sequentialDualSimplex.cpp:119-132) with dotUpdate UPDATE_T set=true.
+    void init_reduced_costs() {
+        std::vector<double> cb(m), y;
+        for (int i = 0; i < m; ++i) cb[i] = costs[basis[i]];
+        btran(cb, y);
+        for (int j : nonbasis) {
+            double acc = 0.0;
+            for (int e = cptr[j]; e < cptr[j + 1]; ++e) acc += cval[e] * y[crow[e]] * -1.0;
+            d[j] = acc + costs[j] * 1.0;
+        }
+    }
+    // dualSimplexInit (sequentialDualSimplex.cpp:230-250)
+    void dual_simplex_init() {
+        set_primal_vars();
+        std::vector<double> buff(N, 0.0), rhs(m), xb;
+        for (int j : nonbasis) buff[j] = x[j];
+        for (int i = 0; i < m; ++i) {
+            double s = 0.0 * 1.0;
+            for (int e = rptr[i]; e < rptr[i + 1]; ++e) s += rval[e] * buff[rcol[e]] * -1.0;
+            rhs[i] = s;
+        }
+        ftran(rhs, xb);
+        for (int i = 0; i < m; ++i) x[basis[i]] = xb[i];
+        init_reduced_costs();
+        double s = 0; for (int j = 0; j < N; ++j) s += costs[j] * x[j];
+        obj = s;
+    }
+    // checkPerturbNeed (tpp:223-234), std::unique semantics kept
+    bool perturb_needed() const {
+        std::vector<double> c(costs);
+        std::sort(c.begin(), c.end());
+        int uniq = c.empty() ? 0 : 1;
+        double last = c.empty() ? 0 : c[0];
+        for (size_t i = 1; i < c.size(); ++i) if (!(std::fabs(last - c[i]) < EPS_COSTS)) { last = c[i]; ++uniq; }
+        return uniq < PERTURB_RATIO * (double)N;
+    }
+    static double weight_for(int i) {  // getWeight (tpp:278-292)
+        static const double w[10] = {0.01, 0.1, 1, 2, 5, 10, 20, 30, 40, 100};
+        int kk = (i > 10) ? 9 : (i == 0 ? 0 : i - 1);
+        return w[kk];
+    }
+    // perturbCosts (tpp:238-275); the sign assignment is overwritten as in the reference
+    void perturb() {
+        original_costs = costs;
+        std::uniform_real_distribution<> dist(0.0, 1.0);
+        double mean = 0; for (double v : costs) mean += v; mean /= (double)N;
+        const double min_p = std::min(1e-2 * EPS_D, PSI);
+        const double max_p = std::max(1e+3 * EPS_D, PSI * 10 * mean);
+        for (int i = 0; i < N; ++i) {
+            const double mag = 100 * EPS_D + PSI * costs[i];
+            double pert;
+            if (type[i] != LOWER && type[i] != FREE) pert = -0.5 * mag * (1 + dist(gen));
+            pert = 0.5 * mag * (1 + dist(gen));
+            pert = weight_for(cptr[i + 1] - cptr[i]) * pert;
+            while (std::fabs(pert) > std::fabs(max_p) || std::fabs(pert) < std::fabs(min_p)) {
+                if (std::fabs(pert) > std::fabs(max_p)) pert = 0.1 * pert;
+                else if (std::fabs(pert) < std::fabs(min_p)) pert = 10 * pert;
+            }
+            costs[i] += pert;
+        }
+        perturbed = true;
+    }
+
+    // pivotRow: Matrix::dotUpdate UPDATE_T, alpha=1, beta=0 (matrix.cpp:273-286)
+    void pivot_row(const std::vector<double>& rho, std::vector<double>& alpha) const {
+        alpha.resize(n);
+        for (int i = 0; i < n; ++i) {
+            const int j = nonbasis[i];
+            double acc = 0.0;
+            for (int e = cptr[j]; e < cptr[j + 1]; ++e) acc += cval[e] * rho[crow[e]] * 1.0;
+            alpha[i] = acc + costs[j] * 0.0;
+        }
+    }
+    // simpleRatioTest (tpp:546-572); q = -1 when nothing is taken (reference: uninitialised)
+    void ratio_test(const std::vector<int>& F, const std::vector<double>& alpha, int& q, int& q_idx) const {
+        q = -1; q_idx = -1;
+        double theta = INF;
+        for (int i : F) {
+            const int j = nonbasis[i];
+            const double tt = d[j] / alpha[i];
+            if (tt < theta) { theta = tt; q = j; q_idx = i; }
+            else if (q_idx >= 0 && std::fabs(tt - theta) < EPS_Z) {
+                if (std::fabs(alpha[i]) > std::fabs(alpha[q_idx])) { theta = tt; q = j; q_idx = i; }
+            }
+        }
+    }
+    void record(int p, int q, double theta) {
+        if (tp && tcount < tcap) { tp[tcount] = p; tq[tcount] = q; tth[tcount] = theta; tob[tcount] = obj; }
+        ++tcount;
+    }
+
+    // ------------------------------------------------------------- phase 1
+    // minimizeDualInfeasibilityInit + initPhase1PricingVector (tpp:776-795,
+    // sequentialDualSimplex.cpp:135-152)
+    void phase1_init(std::vector<double>& f) {
+        init_reduced_costs();
+        std::vector<int> inf_u, inf_l;
+        for (int i = 0; i < n; ++i) {
+            const int j = nonbasis[i];
+            if ((type[j] == UPPER || type[j] == FREE) && d[j] > EPS_D) inf_u.push_back(j);
+            else if ((type[j] == LOWER || type[j] == FREE) && d[j] < -EPS_D) inf_l.push_back(j);
+        }
+        std::vector<double> cc(m, 0.0);
+        double Z = 0;
+        for (int j : inf_l) { Z += d[j]; for (int e = cptr[j]; e < cptr[j + 1]; ++e) cc[crow[e]] += cval[e]; }
+        for (int j : inf_u) { Z -= d[j]; for (int e = cptr[j]; e < cptr[j + 1]; ++e) cc[crow[e]] -= cval[e]; }
+        obj = Z;
+        ftran(cc, f);
+    }
+    // minimizeDualInfeasibility (tpp:799-934)
+    Phase1Out phase1() {
+        in_phase1 = true;
+        Phase1Out st = P1_SOLVED;
+        std::vector<double> rho, f, alpha, alpha_q, tau;
+        phase1_init(f);
+        int cycle = 0;
+        std::unordered_set<int> blocked;
+        long long pivots_at_nop = -1;   // guard: repeated "no row" restart without a pivot
+        while (true) {
+            ++iteration; ++phase1_iters; tick();
+            if (!perturbed && cycle > MAX_CYCLE) { perturb(); phase1_init(f); }
+            if (cycle > NEED_RESTART || obj > INF || std::isnan(obj)) phase1_init(f);
+            if (iteration % opt.refactor_interval == 0) refactor();
+            // phase1Pricing (tpp:746-772)
+            double maxw = 0; int p = -1, p_idx = -1; bool found = false;
+            for (int i = 0; i < m; ++i) {
+                const int j = basis[i];
+                if ((type[j] == LOWER && f[i] > EPS_F) || (type[j] == UPPER && f[i] < -EPS_F) || type[j] == BOXED || type[j] == FIXED) {
+                    const double w = f[i] * f[i] / beta[i];
+                    if (w > maxw && !blocked.count(j)) { p = j; p_idx = i; maxw = w; found = true; }
+                }
+            }
+            const int ndinf = dual_infeasible_count();
+            if (!found || !ndinf) {
+                if (std::fabs(obj) < EPS_A || !ndinf) { st = P1_SOLVED; break; }
+                else if (obj > 0) { st = P1_DUALINF; break; }
+            }
+            if (p < 0 || p_idx < 0) {
+                // The reference's only dual-infeasible exit is obj > 0 (tpp:848), but the
+                // phase-1 objective is a sum of infeasibilities and never positive; with
+                // no leaving row and infeasibilities left the auxiliary problem is at its
+                // optimum, so the LP is dual infeasible (the reference restarts forever).
+                if (!opt.strict_reference && ndinf > 0 && obj < -EPS_A && pivots_at_nop == pivots) { st = P1_DUALINF; break; }
+                pivots_at_nop = pivots;
+                refactor(); phase1_init(f); init_beta(false); blocked.clear(); ++restarts; continue;
+            }
+            if (obj > EPS_BOUND) { refactor(); phase1_init(f); init_beta(false); blocked.clear(); ++restarts; continue; }
+            std::vector<double> e(m, 0.0); e[p_idx] = 1;
+            btran(e, rho);
+            pivot_row(rho, alpha);
+            const bool neg = f[p_idx] > 0;
+            if (neg) for (double& a : alpha) a = -a;
+            std::vector<int> F;  // phase1SetRatioTestCandidates (tpp:530-542)
+            for (int i = 0; i < n; ++i) {
+                const int j = nonbasis[i];
+                if ((d[j] >= 0 && alpha[i] > EPS_A) || (d[j] <= 0 && alpha[i] < -EPS_A)) F.push_back(i);
+            }
+            if (F.empty()) { blocked.insert(p); refactor(); phase1_init(f); ++restarts; continue; }
+            blocked.clear();
+            int q, q_idx;
+            ratio_test(F, alpha, q, q_idx);
+            if (q < 0) { status = ST_ERROR; throw Stop{}; }
+            if (neg) for (double& a : alpha) a = -a;
+            const double theta = d[q] / alpha[q_idx];
+            std::vector<double> aq(m, 0.0);
+            for (int e2 = cptr[q]; e2 < cptr[q + 1]; ++e2) aq[crow[e2]] = cval[e2];
+            ftran(aq, alpha_q);
+            if (std::fabs(alpha_q[p_idx] - alpha[q_idx]) > EPS_R * (1 + std::fabs(alpha_q[p_idx]))) refactor();
+            // infisibilityCorr (tpp:614-625)
+            double corr = 0;
+            if ((type[q] == UPPER || type[q] == FREE) && d[q] > EPS_D) corr = 1;
+            else if ((type[q] == LOWER || type[q] == FREE) && d[q] < -EPS_D) corr = -1;
+            obj = obj - theta * f[p_idx];
+            // simpleReducedCostsUpate (sequentialDualSimplex.cpp:163-172)
+            for (int i = 0; i < n; ++i) { const int j = nonbasis[i]; d[j] -= theta * alpha[i]; }
+            d[p] = -theta; d[q] = 0;
+            const double theta_P = f[p_idx] / alpha_q[p_idx];
+            // phase1UpdateAndChangeBasis (sequentialDualSimplex.cpp:174-197)
+            ftran(rho, tau);
+            std::vector<double> ev(m);
+            const double ap = alpha_q[p_idx], bp = beta[p_idx];
+            for (int i = 0; i < m; ++i) {
+                f[i] = (i != p_idx) ? f[i] - alpha_q[i] * theta_P : f[p_idx];
+                ev[i] = (i != p_idx) ? -alpha_q[i] / ap : 1 / ap;
+                if (i != p_idx) { const double r = alpha_q[i] / ap; beta[i] = beta[i] - 2 * alpha_q[i] / ap * tau[i] + (r * r) * bp; }
+            }
+            beta[p_idx] = beta[p_idx] / (ap * ap);
+            basis[p_idx] = q; nonbasis[q_idx] = p; is_basic[q] = 1; is_basic[p] = 0;
+            eta.push_back(std::move(ev)); eta_p.push_back(p_idx);
+            f[p_idx] = f[p_idx] / alpha_q[p_idx] + corr;
+            ++pivots;
+            cycle = (std::fabs(theta) < EPS_A) ? cycle + 1 : 0;
+        }
+        in_phase1 = false;
+        return st;
+    }
+
+    // ------------------------------------------------------------- phase 2
+    // presolve (tpp:5-30)
+    Phase1Out presolve() {
+        if (perturb_needed()) perturb();
+        init_beta(true);
+        Phase1Out st = phase1();
+        if (st == P1_DUALINF) return st;
+        set_primal_vars();
+        return st;
+    }
+    // callDualSolver (sequentialDualSimplex.cpp:253-515; GPU variant cudaDualSimplex.cpp:396-655)
+    bool phase2() {
+        std::vector<double> rho, alpha, alpha_q, tau, dxb;
+        if (opt.gpu_control_flow) refactor();
+        dual_simplex_init();
+        int cycle = 0;
+        bool unbound_checked = false;
+        long long pivots_at_nop = -1;  // restart-loop guard
+        while (true) {
+            ++iteration; tick();
+            if (iteration % opt.refactor_interval == 0) refactor();
+            if (iteration % NEED_RESTART == 0 && !dual_feasible()) {
+                refactor(); phase1(); dual_simplex_init(); ++restarts;
+            }
+            if (!perturbed && cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); }
+            if (primal_feasible()) { status = ST_OPTIMAL; break; }
+            // DSEPricing (tpp:470-501); blocked set is always empty in phase 2
+            double maxw = 0, delta = 0; int p = -1, p_idx = -1; bool is_lower = false;
+            for (int i = 0; i < m; ++i) {
+                auto [inf, dt] = var_infeas(basis[i]);
+                if (inf && std::fabs(dt) > 1e-8) {
+                    const double w = (dt * dt) / beta[i];
+                    if (w > maxw) { p = basis[i]; p_idx = i; delta = dt; maxw = w; is_lower = dt < 0; }
+                }
+            }
+            if (p < 0 || p_idx < 0) {
+                if (!opt.strict_reference && pivots_at_nop == pivots) {
+                    status = ST_OPTIMAL; break;  // a second restart cannot change anything: infeasibilities <= 1e-8
+                }
+                pivots_at_nop = pivots;
+                refactor(); init_beta(false);
+                if (opt.gpu_control_flow) phase1();
+                dual_simplex_init(); ++restarts;
+                continue;
+            }
+            std::vector<double> e(m, 0.0); e[p_idx] = 1;
+            btran(e, rho);
+            pivot_row(rho, alpha);
+            delta = std::fabs(delta);
+            const int sgn = is_lower ? -1 : 1;
+            if (is_lower) for (double& a : alpha) a = -a;
+            std::vector<int> F; F.reserve(n);
+            for (int i = 0; i < n; ++i) {
+                bool cond = false;
+                const double a = alpha[i];
+                const int j = nonbasis[i];
+                if (a > EPS_A) cond = std::fabs(x[j] - lb[j]) < EPS_Z && (type[j] == LOWER || type[j] == BOXED);
+                else if (a < -EPS_A) cond = std::fabs(x[j] - ub[j]) < EPS_Z && (type[j] == UPPER || type[j] == BOXED);
+                else cond = type[j] == FREE;
+                if (cond) F.push_back(i);
+            }
+            if (F.empty()) {
+                if (unbound_checked) { status = ST_PRIMAL_INF; break; }
+                unbound_checked = true;
+                refactor(); init_beta(false); phase1(); dual_simplex_init(); ++restarts;
+                continue;
+            }
+            unbound_checked = false;
+            int q = -1, q_idx = -1;
+            while (!F.empty()) {
+                ratio_test(F, alpha, q, q_idx);
+                if (q < 0) break;
+                if (type[q] == BOXED) {
+                    if (delta - (ub[q] - lb[q]) * std::fabs(alpha[q_idx]) <= 0) break;
+                    delta -= (ub[q] - lb[q]) * std::fabs(alpha[q_idx]);
+                    F.erase(std::remove(F.begin(), F.end(), q_idx), F.end());
+                } else break;
+            }
+            if (q < 0) { status = ST_ERROR; throw Stop{}; }
+            if (is_lower) for (double& a : alpha) a = -a;
+            const double theta = d[q] / alpha[q_idx];
+            delta = sgn * delta;
+            std::vector<double> aq(m, 0.0);
+            for (int e2 = cptr[q]; e2 < cptr[q + 1]; ++e2) aq[crow[e2]] = cval[e2];
+            ftran(aq, alpha_q);
+            if (std::fabs(alpha_q[p_idx] - alpha[q_idx]) > EPS_R * (1 + std::fabs(alpha_q[p_idx]))) refactor();
+            // dual update + BFRT sets (sequentialDualSimplex.cpp:438-467)
+            std::vector<int> low, up;
+            std::vector<double> cc(m, 0.0);
+            double dz = 0;
+            for (int i = 0; i < n; ++i) {
+                const int j = nonbasis[i];
+                d[j] = d[j] - theta * alpha[i];
+                if (type[j] == BOXED) {
+                    if (std::fabs(x[j] - lb[j]) < EPS_Z && d[j] < -EPS_D) { low.push_back(j); dz += costs[j] * (ub[j] - lb[j]); }
+                    else if (std::fabs(x[j] - ub[j]) < EPS_Z && d[j] > EPS_D) { up.push_back(j); dz -= costs[j] * (ub[j] - lb[j]); }
+                }
+            }
+            for (int j : low) for (int e2 = cptr[j]; e2 < cptr[j + 1]; ++e2) cc[crow[e2]] += cval[e2] * diff_bounds[j] * 1.0;
+            for (int j : up) for (int e2 = cptr[j]; e2 < cptr[j + 1]; ++e2) cc[crow[e2]] += cval[e2] * diff_bounds[j] * -1.0;
+            d[p] = -theta; d[q] = 0;
+            if (!up.empty() || !low.empty()) {
+                ftran(cc, dxb);
+                for (int i = 0; i < m; ++i) x[basis[i]] = x[basis[i]] - dxb[i];
+                for (int i = 0; i < m; ++i) dz -= costs[basis[i]] * dxb[i];
+                flips += (int)(low.size() + up.size());
+            }
+            obj += dz;
+            const double theta_P = delta / alpha_q[p_idx];
+            // updateAndChangeBasis (sequentialDualSimplex.cpp:200-227)
+            ftran(rho, tau);
+            std::vector<double> ev(m);
+            const double ap = alpha_q[p_idx], bp = beta[p_idx];
+            for (int i = 0; i < m; ++i) {
+                const int j = basis[i];
+                x[j] = x[j] - theta_P * alpha_q[i];
+                ev[i] = (i != p_idx) ? -alpha_q[i] / ap : 1 / ap;
+                if (i != p_idx) { const double r = alpha_q[i] / ap; beta[i] = beta[i] - 2 * alpha_q[i] / ap * tau[i] + (r * r) * bp; }
+            }
+            beta[p_idx] = beta[p_idx] / (ap * ap);
+            x[q] = x[q] + theta_P;
+            basis[p_idx] = q; nonbasis[q_idx] = p; is_basic[q] = 1; is_basic[p] = 0;
+            eta.push_back(std::move(ev)); eta_p.push_back(p_idx);
+            for (int j : low) x[j] = ub[j];
+            for (int j : up) x[j] = lb[j];
+            obj += theta * delta;
+            if (std::fabs(theta) < EPS_A) cycle += 1;
+            ++pivots;
+            record(p, q, theta);
+        }
+        return status == ST_OPTIMAL;
+    }
+    // presolve + solve + postProcess (tpp:123-180), with the optional cleanup
+    void run() {
+        try {
+            refactor();  // initDualSimplex: B <- slack basis, LU (sequentialDualSimplex.cpp:4-25)
+            Phase1Out st = presolve();
+            if (st == P1_DUALINF) { status = ST_DUAL_INF; return; }
+            bool ok = phase2();
+            for (int round = 0; round < 3 && perturbed; ++round) {
+                costs = original_costs;
+                dual_simplex_init();
+                if (!ok || opt.strict_reference || dual_feasible()) break;
+                // cleanup: the perturbed optimum is dual infeasible for the true costs
+                status = ST_UNSOLVED;
+                refactor(); Phase1Out s1 = phase1();
+                if (s1 == P1_DUALINF) { status = ST_DUAL_INF; return; }
+                set_primal_vars();
+                ok = phase2();
+            }
+        } catch (const Stop&) {
+            if (status == ST_UNSOLVED || status == ST_OPTIMAL) status = ST_ERROR;
+        }
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+void or_default_options(or_options* o) {
+    o->refactor_interval = 100;
+    o->max_iterations = 2000000;
+    o->strict_reference = 0;
+    o->seed = 12345;
+    o->gpu_control_flow = 1;
+    o->verbose = 0;
+}
+
+int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,
+                   const double* c, const int* col_type, const double* col_lb, const double* col_ub,
+                   const int* row_type, const double* row_lb, const double* row_ub,
+                   const or_options* opt, or_result* res, double* x_out, double* d_out,
+                   int* basis_out, int* trace_p, int* trace_q, double* trace_theta,
+                   double* trace_obj, int trace_cap, int* trace_count) {
+    if (m <= 0 || n <= 0 || !row_ptr || !res) return -1;
+    if (m > n) return -4;  // Problem::checkConstraints (problem.tpp:230-239)
+    Oracle o;
+    if (opt) o.opt = *opt; else or_default_options(&o.opt);
+    o.load(m, n, row_ptr, col_idx, val, c, col_type, col_lb, col_ub, row_type, row_lb, row_ub);
+    o.tp = trace_p; o.tq = trace_q; o.tth = trace_theta; o.tob = trace_obj; o.tcap = trace_cap;
+    o.run();
+    res->status = o.status;
+    res->iterations = o.iteration;
+    res->phase1_iterations = o.phase1_iters;
+    res->refactors = o.refactors;
+    res->restarts = o.restarts;
+    res->perturbed = o.perturbed;
+    res->bfrt_flips = o.flips;
+    res->bump_size = o.k;
+    double z = 0; for (int j = 0; j < n; ++j) z += (o.perturbed ? o.original_costs[j] : o.costs[j]) * o.x[j];
+    res->objective = z;
+    res->obj_incremental = o.obj;
+    if (x_out) std::memcpy(x_out, o.x.data(), sizeof(double) * o.N);
+    if (d_out) std::memcpy(d_out, o.d.data(), sizeof(double) * o.N);
+    if (basis_out) std::memcpy(basis_out, o.basis.data(), sizeof(int) * m);
+    if (trace_count) *trace_count = o.tcount;
+    return 0;
+}
+
+int or_dse_pricing(int m, const int* basis, const double* x, const double* lb, const double* ub,
+                   const int* type, const double* beta, int* p, int* p_idx, double* delta,
+                   int* is_lower, int* primal_feasible) {
+    // Same code path as the solver: a tiny Oracle holding only the vectors.
+    Oracle o;
+    int N = 0;
+    for (int i = 0; i < m; ++i) N = std::max(N, basis[i] + 1);
+    (void)N;
+    o.m = m;
+    // DSEPricing (tpp:470-501) on caller vectors
+    double maxw = 0, dl = 0; int pp = -1, pi = -1; bool il = false;
+    auto infeas = [&](int i) -> std::pair<bool, double> {
+        switch (type[i]) {
+            case LOWER: if (x[i] < lb[i] - EPS_BOUND) return {true, x[i] - lb[i]}; [[fallthrough]];
+            case UPPER: if (x[i] > ub[i] + EPS_BOUND) return {true, x[i] - ub[i]}; [[fallthrough]];
+            case FIXED: if (std::fabs(x[i] - lb[i]) < EPS_BOUND) return {true, x[i] - lb[i]}; [[fallthrough]];
+            case BOXED:
+                if (x[i] > ub[i] + EPS_BOUND) return {true, x[i] - ub[i]};
+                else if (x[i] < lb[i] - EPS_BOUND) return {true, x[i] - lb[i]};
+        }
+        return {false, 0.0};
+    };
+    for (int i = 0; i < m; ++i) {
+        auto [inf, dt] = infeas(basis[i]);
+        if (inf && std::fabs(dt) > 1e-8) {
+            const double w = (dt * dt) / beta[i];
+            if (w > maxw) { pp = basis[i]; pi = i; dl = dt; maxw = w; il = dt < 0; }
+        }
+    }
+    *p = pp; *p_idx = pi; *delta = dl; *is_lower = il;
+    bool feas = true;
+    for (int ii = 0; ii < m && feas; ++ii) {
+        const int i = basis[ii];
+        switch (type[i]) {
+            case FIXED: if (std::fabs(x[i] - lb[i]) > EPS_BOUND) { feas = false; break; } [[fallthrough]];
+            case FREE: break;
+            case BOXED:
+                if (x[i] > ub[i] + EPS_R * std::fabs(ub[i]) + EPS_BOUND || x[i] < lb[i] - EPS_R * std::fabs(lb[i]) - EPS_BOUND) { feas = false; break; }
+                [[fallthrough]];
+            case UPPER: if (x[i] > ub[i] + EPS_R * std::fabs(ub[i]) + EPS_BOUND) { feas = false; break; } [[fallthrough]];
+            case LOWER: if (x[i] < lb[i] - EPS_R * std::fabs(lb[i]) - EPS_BOUND) { feas = false; break; }
+        }
+    }
+    *primal_feasible = feas;
+    return 0;
+}
+
+int or_ratio_test(int n, const int* nonbasis, const double* alpha_in, double delta_in, int is_lower,
+                  const double* x, const double* d, const double* lb, const double* ub,
+                  const int* type, int* q_out, int* q_idx_out, double* theta_out, double* delta_out,
+                  int* num_candidates) {
+    std::vector<double> alpha(alpha_in, alpha_in + n);
+    double delta = std::fabs(delta_in);
+    const int sgn = is_lower ? -1 : 1;
+    if (is_lower) for (double& a : alpha) a = -a;
+    std::vector<int> F;
+    for (int i = 0; i < n; ++i) {
+        bool cond = false;
+        const double a = alpha[i];
+        const int j = nonbasis[i];
+        if (a > EPS_A) cond = std::fabs(x[j] - lb[j]) < EPS_Z && (type[j] == LOWER || type[j] == BOXED);
+        else if (a < -EPS_A) cond = std::fabs(x[j] - ub[j]) < EPS_Z && (type[j] == UPPER || type[j] == BOXED);
+        else cond = type[j] == FREE;
+        if (cond) F.push_back(i);
+    }
+    *num_candidates = (int)F.size();
+    int q = -1, q_idx = -1;
+    auto scan = [&]() {
+        q = -1; q_idx = -1;
+        double theta = INF;
+        for (int i : F) {
+            const int j = nonbasis[i];
+            const double tt = d[j] / alpha[i];
+            if (tt < theta) { theta = tt; q = j; q_idx = i; }
+            else if (q_idx >= 0 && std::fabs(tt - theta) < EPS_Z) {
+                if (std::fabs(alpha[i]) > std::fabs(alpha[q_idx])) { theta = tt; q = j; q_idx = i; }
+            }
+        }
+    };
+    while (!F.empty()) {
+        scan();
+        if (q < 0) break;
+        if (type[q] == BOXED) {
+            if (delta - (ub[q] - lb[q]) * std::fabs(alpha[q_idx]) <= 0) break;
+            delta -= (ub[q] - lb[q]) * std::fabs(alpha[q_idx]);
+            F.erase(std::remove(F.begin(), F.end(), q_idx), F.end());
+        } else break;
+    }
+    *q_out = q; *q_idx_out = q_idx;
+    if (q >= 0) {
+        *theta_out = d[q] / alpha_in[q_idx];
+    } else {
+        *theta_out = 0;
+    }
+    *delta_out = sgn * delta;
+    return 0;
+}
+
+int or_pivot_row(int m, int n, const int* csc_ptr, const int* csc_row, const double* csc_val,
+                 const int* nonbasis, const double* rho, double* alpha) {
+    (void)m;
+    for (int i = 0; i < n; ++i) {
+        const int j = nonbasis[i];
+        double acc = 0.0;
+        if (j < n) {
+            for (int e = csc_ptr[j]; e < csc_ptr[j + 1]; ++e) acc += csc_val[e] * rho[csc_row[e]] * 1.0;
+        } else {
+            acc += 1.0 * rho[j - n] * 1.0;
+        }
+        alpha[i] = acc;
+    }
+    return 0;
+}
+
+int or_pfi_apply(int m, int T, const double* etav, const int* pos, const double* rhs, double* sol,
+                 int transpose) {
+    std::vector<double> s(rhs, rhs + m);
+    if (!transpose) {
+        for (int t = 0; t < T; ++t) {
+            const int kk = pos[t]; const double* ev = etav + (size_t)t * m;
+            const double sk = s[kk];
+            for (int i = 0; i < m; ++i) s[i] = s[i] + sk * ev[i];
+            s[kk] = sk * ev[kk];
+        }
+    } else {
+        for (int t = T - 1; t >= 0; --t) {
+            const int kk = pos[t]; const double* ev = etav + (size_t)t * m;
+            double acc = 0.0;
+            for (int i = 0; i < m; ++i) acc += ev[i] * s[i];
+            s[kk] = acc;
+        }
+    }
+    std::memcpy(sol, s.data(), sizeof(double) * m);
+    return 0;
+}
+
+int or_dense_solve(int n, const int* csr_ptr, const int* csr_col, const double* csr_val,
+                   const double* rhs, double* sol, int transpose) {
+    std::vector<double> A((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int e = csr_ptr[i]; e < csr_ptr[i + 1]; ++e) A[(size_t)i * n + csr_col[e]] = csr_val[e];
+    if (transpose)
+        for (int i = 0; i < n; ++i) for (int j = i + 1; j < n; ++j) std::swap(A[(size_t)i * n + j], A[(size_t)j * n + i]);
+    std::vector<double> b(rhs, rhs + n);
+    for (int c = 0; c < n; ++c) {
+        int pr = c; double best = std::fabs(A[(size_t)c * n + c]);
+        for (int r = c + 1; r < n; ++r) if (std::fabs(A[(size_t)r * n + c]) > best) { best = std::fabs(A[(size_t)r * n + c]); pr = r; }
+        if (!(best > 0)) return -5;
+        if (pr != c) { for (int j = 0; j < n; ++j) std::swap(A[(size_t)c * n + j], A[(size_t)pr * n + j]); std::swap(b[c], b[pr]); }
+        for (int r = c + 1; r < n; ++r) {
+            const double l = A[(size_t)r * n + c] / A[(size_t)c * n + c];
+            for (int j = c; j < n; ++j) A[(size_t)r * n + j] -= l * A[(size_t)c * n + j];
+            b[r] -= l * b[c];
+        }
+    }
+    for (int r = n - 1; r >= 0; --r) {
+        double s = b[r];
+        for (int j = r + 1; j < n; ++j) s -= A[(size_t)r * n + j] * sol[j];
+        sol[r] = s / A[(size_t)r * n + r];
+    }
+    return 0;
+}
+
+}  // extern "C"

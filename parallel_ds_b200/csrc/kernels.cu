@@ -1,0 +1,1267 @@
+// Per-iteration kernels of the dual simplex hot loop (sm_100a, FP64).
+//
+// One iteration (reference: CudaDualSimplex::callDualSolver,
+// cudaDualSimplex.cpp:417-648) is this launch sequence, captured once per
+// factor as a CUDA graph:
+//
+//   k_top          loop bookkeeping: iteration++, refactor / restart / perturb
+//   k_dual_check   checkDualFeasible every NEED_RESTART iterations
+//   k_chuzr        CHUZR (DSE pricing + optimality test), then the eta part of
+//                  BTRAN for e_p in the last block
+//   k_btran_rhs    BTRAN through the basis's slack rows
+//   k_btran_gemv   BTRAN through Kinv^T -> rho
+//   k_pivot_row    alpha_N = rho^T A_N fused with CHUZC part 1; the last block
+//                  runs CHUZC part 2 (ordered tie scan) and the BFRT loop
+//   k_dual_update  d_N -= theta alpha_N, bound-flip set, BFRT column change
+//   k_ftran_k      FTRAN through Kinv for [a_q, rho, column_change] at once
+//   k_ftran_assemble  FTRAN through the slack rows; eta-chain scalars s = M g
+//   k_eta_apply    y = y0 + sum_t s_t (eta_t - e_{p_t}) in one streaming pass
+//   k_update       x_B, DSE weights, eta append, basis swap, flips, objective
+//
+// A kernel that needs a decision reads it from Ctl; any kernel may raise an
+// event, after which every later kernel of the iteration returns at once and
+// the host handles the event.  "Last block" finishing uses a ticket counter
+// (threadfence + atomicAdd); all reductions are in a fixed order, so results
+// do not depend on scheduling.
+//
+// Arithmetic that decides indices follows the reference's operation order
+// exactly and the file is compiled with -fmad=false.
+#include <cfloat>
+#include <climits>
+#include <cmath>
+
+#include <math_constants.h>
+
+#include "engine.cuh"
+#include "kernels.cuh"
+
+namespace ds {
+
+__device__ __forceinline__ bool halted(const Ctl* c) { return *(volatile const int*)&c->halt != 0; }
+
+__device__ __forceinline__ void raise_ev(Ctl* c, int ev, int stage) {
+    c->event = ev;
+    c->event_stage = stage;
+    c->halt = 1;
+    __threadfence();
+}
+
+// True in exactly one block: the last one to arrive.  All blocks must call it.
+__device__ bool last_block(unsigned* ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned nb = gridDim.x * gridDim.y;
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == nb - 1);
+        if (is_last) *ticket = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// ---------------------------------------------------------------- reductions
+struct ArgMax { double w; int i; };
+__device__ __forceinline__ ArgMax better_max(ArgMax a, ArgMax b) {  // larger w, then smaller i
+    if (b.w > a.w || (b.w == a.w && b.i < a.i)) return b;
+    return a;
+}
+struct ArgMin { double t; int i; };
+__device__ __forceinline__ ArgMin better_min(ArgMin a, ArgMin b) {  // smaller t, then smaller i
+    if (b.t < a.t || (b.t == a.t && b.i < a.i)) return b;
+    return a;
+}
+
+template <int BS>
+__device__ ArgMax block_argmax(ArgMax v) {
+    __shared__ double sw[BS / 32];
+    __shared__ int si[BS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        ArgMax u{__shfl_down_sync(0xffffffffu, v.w, o), __shfl_down_sync(0xffffffffu, v.i, o)};
+        v = better_max(v, u);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sw[wid] = v.w; si[wid] = v.i; }
+    __syncthreads();
+    if (wid == 0) {
+        v = (lane < BS / 32) ? ArgMax{sw[lane], si[lane]} : ArgMax{-1.0, INT_MAX};
+        for (int o = 16; o > 0; o >>= 1) {
+            ArgMax u{__shfl_down_sync(0xffffffffu, v.w, o), __shfl_down_sync(0xffffffffu, v.i, o)};
+            v = better_max(v, u);
+        }
+    }
+    __syncthreads();
+    return v;  // valid in thread 0
+}
+
+template <int BS>
+__device__ ArgMin block_argmin(ArgMin v) {
+    __shared__ double st[BS / 32];
+    __shared__ int si[BS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        ArgMin u{__shfl_down_sync(0xffffffffu, v.t, o), __shfl_down_sync(0xffffffffu, v.i, o)};
+        v = better_min(v, u);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { st[wid] = v.t; si[wid] = v.i; }
+    __syncthreads();
+    if (wid == 0) {
+        v = (lane < BS / 32) ? ArgMin{st[lane], si[lane]} : ArgMin{CUDART_INF, INT_MAX};
+        for (int o = 16; o > 0; o >>= 1) {
+            ArgMin u{__shfl_down_sync(0xffffffffu, v.t, o), __shfl_down_sync(0xffffffffu, v.i, o)};
+            v = better_min(v, u);
+        }
+    }
+    __syncthreads();
+    return v;
+}
+
+template <int BS>
+__device__ int block_sum_int(int v) {
+    __shared__ int s[BS / 32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = (lane < BS / 32) ? s[lane] : 0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+template <int BS>
+__device__ double block_sum(double v) {
+    __shared__ double s[BS / 32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) s[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = (lane < BS / 32) ? s[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+// ------------------------------------------------------------ per-variable rules
+// checkVarIsInfeas (baseDualSimplex.tpp:443-466) with its case fallthrough.
+__device__ __forceinline__ bool var_infeas(unsigned char t, double x, double l, double u, double* delta) {
+    switch (t) {
+        case LOWER:
+            if (x < l - EPS_BOUND) { *delta = x - l; return true; }
+            [[fallthrough]];
+        case UPPER:
+            if (x > u + EPS_BOUND) { *delta = x - u; return true; }
+            [[fallthrough]];
+        case FIXED:
+            if (fabs(x - l) < EPS_BOUND) { *delta = x - l; return true; }
+            [[fallthrough]];
+        case BOXED:
+            if (x > u + EPS_BOUND) { *delta = x - u; return true; }
+            else if (x < l - EPS_BOUND) { *delta = x - l; return true; }
+    }
+    *delta = 0.0;
+    return false;
+}
+
+// checkPrimalFeasible (tpp:296-324) for one basic variable, fallthrough kept.
+__device__ __forceinline__ bool var_primal_ok(unsigned char t, double x, double l, double u) {
+    switch (t) {
+        case FIXED:
+            if (fabs(x - l) > EPS_BOUND) return false;
+            [[fallthrough]];
+        case FREE: return true;
+        case BOXED:
+            if (x > u + EPS_R * fabs(u) + EPS_BOUND || x < l - EPS_R * fabs(l) - EPS_BOUND) return false;
+            [[fallthrough]];
+        case UPPER:
+            if (x > u + EPS_R * fabs(u) + EPS_BOUND) return false;
+            [[fallthrough]];
+        case LOWER:
+            if (x < l - EPS_R * fabs(l) - EPS_BOUND) return false;
+    }
+    return true;
+}
+
+// checkDualFeasible (tpp:362-385) for one nonbasic variable.
+__device__ __forceinline__ bool var_dual_bad(unsigned char t, double d) {
+    switch (t) {
+        case FREE: return fabs(d) < EPS_D || isnan(d);
+        case UPPER: return d > EPS_D || isnan(d);
+        case LOWER: return d < -EPS_D || isnan(d);
+        default: return false;
+    }
+}
+
+// simpleRatioTestPart1 candidate rule (cudaDualSimplex.cpp:367-394).
+__device__ __forceinline__ bool rt_candidate(double a, unsigned char t, double x, double l, double u) {
+    if (a > EPS_A) return fabs(x - l) < EPS_Z && (t == LOWER || t == BOXED);
+    if (a < -EPS_A) return fabs(x - u) < EPS_Z && (t == UPPER || t == BOXED);
+    return t == FREE;
+}
+
+// ======================================================================= top
+__global__ void k_top(Dev D) {
+    Ctl* c = D.ctl;
+    if (threadIdx.x != 0 || halted(c)) return;
+    const int it = ++c->iteration;
+    if (it > c->max_iter) { raise_ev(c, EV_ITER_LIMIT, ST_TOP); return; }
+    if (it % c->R == 0) { raise_ev(c, EV_REFACTOR_DUE, ST_TOP); return; }
+    c->need_dual_check = (it % NEED_RESTART == 0);
+    c->dual_infeas = 0;
+    if (!c->need_dual_check && !c->perturbed && c->cycle > MAX_CYCLE) raise_ev(c, EV_PERTURB, ST_TOP);
+}
+
+// checkDualFeasible over the nonbasic slots; also used standalone (force=1).
+template <int BS>
+__global__ void k_dual_check(Dev D, int force) {
+    Ctl* c = D.ctl;
+    if (!force && (halted(c) || !c->need_dual_check)) return;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    int bad = 0;
+    if (i < D.n) {
+        const int j = D.nonbasis[i];
+        bad = var_dual_bad(D.type[j], D.d[j]) ? 1 : 0;
+    }
+    bad = block_sum_int<BS>(bad);
+    if (threadIdx.x == 0 && bad) atomicAdd(&c->dual_infeas, bad);
+    if (last_block(&c->tickets[1]) && threadIdx.x == 0) {
+        if (force) return;
+        c->need_dual_check = 0;
+        if (c->dual_infeas > 0) raise_ev(c, EV_DUALINF, ST_TOP);
+        else if (!c->perturbed && c->cycle > MAX_CYCLE) raise_ev(c, EV_PERTURB, ST_TOP);
+    }
+}
+
+// ====================================================================== CHUZR
+// Eta part of BTRAN for the unit vector e_p, run by one block:
+//   h_t = eta_t[p] - [p_t == p],  delta = Mtri^T h,  y = e_p + sum_t delta_t e_{p_t}.
+// (Mtri = (I - G)^-1 with G[t][u] = eta_u[p_t] - [p_u == p_t] for u < t.)
+template <int BS>
+__device__ void btran_unit_eta(const Dev& D, int p_idx) {
+    Ctl* c = D.ctl;
+    __shared__ double h[1024];
+    __shared__ double dl[1024];
+    const int T = c->T;
+    // clear what the previous BTRAN left in ybt
+    const int nprev = c->ybt_n;
+    if (nprev < 0) {
+        for (int i = threadIdx.x; i < D.m; i += BS) D.ybt[i] = 0.0;
+    } else {
+        for (int u = threadIdx.x; u < nprev; u += BS) D.ybt[D.ybt_pos[u]] = 0.0;
+    }
+    for (int t = threadIdx.x; t < T; t += BS)
+        h[t] = D.eta[(size_t)t * D.m + p_idx] - (D.eta_pos[t] == p_idx ? 1.0 : 0.0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < T; t += BS) {
+        double s = 0.0;
+        for (int v = t; v < T; ++v) s += D.Mtri[(size_t)v * D.cap + t] * h[v];
+        dl[t] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        D.ybt[p_idx] = 1.0;
+        D.ybt_pos[0] = p_idx;
+        for (int t = 0; t < T; ++t) {
+            const int pt = D.eta_pos[t];
+            D.ybt[pt] = D.ybt[pt] + dl[t];
+            D.ybt_pos[t + 1] = pt;
+        }
+        c->ybt_n = T + 1;
+    }
+    __syncthreads();
+}
+
+// DSEPricing (tpp:470-501) + checkPrimalFeasible (tpp:296-324), or phase1Pricing
+// (tpp:746-772) when Ctl::phase == 1.
+template <int BS>
+__global__ void k_chuzr(Dev D) {
+    Ctl* c = D.ctl;
+    if (halted(c)) return;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    const int phase = c->phase;
+    ArgMax best{-1.0, INT_MAX};
+    int infeas = 0;
+    if (i < D.m) {
+        const int j = D.basis[i];
+        const unsigned char t = D.type[j];
+        if (phase == 2) {
+            const double x = D.x[j], l = D.lb[j], u = D.ub[j];
+            double dt;
+            if (var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8) {
+                const double w = (dt * dt) / D.beta[i];
+                if (w > 0.0) best = ArgMax{w, i};   // strict '>' against max_weight = 0; NaN never wins
+            }
+            infeas = var_primal_ok(t, x, l, u) ? 0 : 1;
+        } else {
+            const double fi = D.f[i];
+            if ((t == LOWER && fi > EPS_F) || (t == UPPER && fi < -EPS_F) || t == BOXED || t == FIXED) {
+                const double w = (fi * fi) / D.beta[i];
+                if (w > 0.0 && !D.blocked[j]) best = ArgMax{w, i};
+            }
+        }
+    }
+    best = block_argmax<BS>(best);
+    infeas = block_sum_int<BS>(infeas);
+    if (threadIdx.x == 0) {
+        D.red[blockIdx.x] = best.w;
+        D.redi[blockIdx.x] = best.i;
+        D.redi[gridDim.x + blockIdx.x] = infeas;
+    }
+    if (!last_block(&c->tickets[2])) return;
+    // ---- last block: combine the partials in block order
+    __shared__ int s_pidx;
+    ArgMax v{-1.0, INT_MAX};
+    int tot = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
+        v = better_max(v, ArgMax{D.red[b], D.redi[b]});
+        tot += D.redi[gridDim.x + b];
+    }
+    v = block_argmax<BS>(v);
+    tot = block_sum_int<BS>(tot);
+    if (threadIdx.x == 0) {
+        s_pidx = -1;
+        const int pidx = (v.i == INT_MAX || v.w <= 0.0) ? -1 : v.i;
+        if (phase == 2) {
+            c->primal_feasible = (tot == 0);
+            c->p = -1; c->p_idx = -1;
+            if (pidx >= 0) {
+                const int j = D.basis[pidx];
+                double dt;
+                var_infeas(D.type[j], D.x[j], D.lb[j], D.ub[j], &dt);
+                c->p = j; c->p_idx = pidx; c->delta = dt; c->is_lower = dt < 0;
+                c->beta_p = D.beta[pidx];
+            }
+            if (tot == 0) raise_ev(c, EV_OPTIMAL, ST_PRICING);
+            else if (pidx < 0) raise_ev(c, EV_NO_P, ST_PRICING);
+            else s_pidx = pidx;
+        } else {
+            const int found = pidx >= 0;
+            c->p1_found = found;
+            const int dinf = c->p1_dinf;
+            const double Z = c->z_phase1;
+            int ev = EV_NONE;
+            if (!found || !dinf) {
+                if (fabs(Z) < EPS_A || !dinf) ev = EV_P1_DONE;
+                else if (Z > 0) ev = EV_P1_DUALINF;
+            }
+            if (ev == EV_NONE && pidx < 0) ev = EV_P1_RESTART;
+            if (ev == EV_NONE && Z > EPS_BOUND) ev = EV_P1_RESTART;
+            if (ev != EV_NONE) raise_ev(c, ev, ST_PRICING);
+            else {
+                c->p = D.basis[pidx]; c->p_idx = pidx; c->f_p = D.f[pidx];
+                c->beta_p = D.beta[pidx];
+                s_pidx = pidx;
+            }
+        }
+    }
+    __syncthreads();
+    if (s_pidx >= 0) btran_unit_eta<BS>(D, s_pidx);
+}
+
+// Standalone eta part of BTRAN for e_{p_idx} (exact DSE weight recomputation).
+template <int BS>
+__global__ void k_btran_unit(Dev D, int p_idx) { btran_unit_eta<BS>(D, p_idx); }
+
+// ====================================================================== BTRAN
+// rhs_j = y[s_pos[j]] - sum_{r in col(s_var[j]), r in R} a_rj * y[slackpos(r)]
+template <int BS>
+__global__ void k_btran_rhs(Dev D, int force) {
+    if (!force && halted(D.ctl)) return;
+    const int j = blockIdx.x * BS + threadIdx.x;
+    if (j >= D.k) return;
+    const int v = D.s_var[j];
+    double s = D.ybt[D.s_pos[j]];
+    for (int e = D.cptr[v]; e < D.cptr[v + 1]; ++e) {
+        const int sp = D.row_slackpos[D.crow[e]];
+        if (sp >= 0) s -= D.cval[e] * D.ybt[sp];
+    }
+    D.btr_rhs[j] = s;
+}
+
+// rho[rp_row[t]] = sum_j Kinv(j, t) rhs_j (one warp per t), rho[r] = y[slackpos(r)] for r in R.
+template <int BS>
+__global__ void k_btran_gemv(Dev D, double* out, int force) {
+    if (!force && halted(D.ctl)) return;
+    const int warps_per_block = BS / 32;
+    const int nb_warp = (D.k + warps_per_block - 1) / warps_per_block;
+    if ((int)blockIdx.x < nb_warp) {
+        const int t = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        if (t >= D.k) return;
+        const double* col = D.Kinv + (size_t)t * D.k;
+        double s = 0.0;
+        for (int j = lane; j < D.k; j += 32) s += col[j] * D.btr_rhs[j];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) out[D.rp_row[t]] = s;
+    } else {
+        const int r = (blockIdx.x - nb_warp) * BS + threadIdx.x;
+        if (r >= D.m) return;
+        const int sp = D.row_slackpos[r];
+        if (sp >= 0) out[r] = D.ybt[sp];
+    }
+}
+
+// ================================================================ pivot row
+// Full sequential ratio scan over F in slot order (simpleRatioTest, tpp:546-572):
+// the fallback when the tie window could not be shown exact.
+__device__ void rt_full_scan(const Dev& D, double sgn_a, int* q_idx_out) {
+    double theta = INF_THETA;
+    int q_idx = -1;
+    for (int i = 0; i < D.n; ++i) {
+        if (!D.cand[i]) continue;
+        const double th = D.theta_arr[i];
+        if (isnan(th)) continue;   // removed by BFRT or not takeable
+        const double a = sgn_a * D.alpha[i];
+        if (th < theta) { theta = th; q_idx = i; }
+        else if (q_idx >= 0 && fabs(th - theta) < EPS_Z) {
+            if (fabs(a) > fabs(sgn_a * D.alpha[q_idx])) { theta = th; q_idx = i; }
+        }
+    }
+    *q_idx_out = q_idx;
+}
+
+// CHUZC part 2 from the first minimiser (theta*, i*): the sequential scan's state
+// after i* is (theta*, i*) whatever came before, and later candidates can only be
+// taken through the EPS_Z tie branch, i.e. from a chain starting at theta*.  The
+// chain is followed over the candidates inside [theta*, theta* + RT_WINDOW]; if it
+// stayed at least 2 EPS_Z below the window edge no outside candidate could have
+// joined it and the result equals the full scan; otherwise the full scan runs.
+template <int BS>
+__device__ int rt_select(const Dev& D, double sgn_a) {
+    __shared__ double s_tmin[BS / 32];
+    __shared__ int s_imin[BS / 32];
+    __shared__ int list[2048];
+    __shared__ int nlist, overflow, result;
+    __shared__ double s_bound;
+    // global first minimiser over takeable candidates
+    ArgMin v{CUDART_INF, INT_MAX};
+    for (int i = threadIdx.x; i < D.n; i += BS) {
+        const double th = D.theta_arr[i];
+        if (D.cand[i] && !isnan(th)) v = better_min(v, ArgMin{th, i});
+    }
+    (void)s_tmin; (void)s_imin;
+    v = block_argmin<BS>(v);
+    if (threadIdx.x == 0) {
+        nlist = 0; overflow = 0; result = (v.i == INT_MAX) ? -1 : v.i;
+        s_bound = v.t + RT_WINDOW;
+        s_tmin[0] = v.t;
+    }
+    __syncthreads();
+    if (result < 0) return -1;
+    const int istar = result;
+    const double B = s_bound;
+    // ordered collection of window members after i*
+    for (int base = istar + 1; base < D.n; base += BS) {
+        const int i = base + threadIdx.x;
+        bool mem = false;
+        if (i < D.n && D.cand[i]) {
+            const double th = D.theta_arr[i];
+            mem = !isnan(th) && th <= B;
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, mem);
+        __shared__ int wcount[BS / 32];
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) wcount[wid] = __popc(ball);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = nlist;
+            for (int w = 0; w < BS / 32; ++w) { const int cnt = wcount[w]; wcount[w] = acc; acc += cnt; }
+            if (acc > 2048) overflow = 1;
+            nlist = acc > 2048 ? 2048 : acc;
+        }
+        __syncthreads();
+        if (mem) {
+            const int slot = wcount[wid] + __popc(ball & ((1u << lane) - 1u));
+            if (slot < 2048) list[slot] = i;
+        }
+        __syncthreads();
+        if (overflow) break;
+    }
+    if (threadIdx.x == 0) {
+        int q = istar;
+        double theta = D.theta_arr[istar];
+        double maxrun = theta;
+        bool exact = !overflow;
+        if (exact) {
+            for (int u = 0; u < nlist; ++u) {
+                const int i = list[u];
+                const double th = D.theta_arr[i];
+                const double a = sgn_a * D.alpha[i];
+                if (th < theta) { theta = th; q = i; }
+                else if (fabs(th - theta) < EPS_Z) {
+                    if (fabs(a) > fabs(sgn_a * D.alpha[q])) { theta = th; q = i; }
+                }
+                if (theta > maxrun) maxrun = theta;
+            }
+            exact = (B - maxrun) >= 2.0 * EPS_Z;
+        }
+        if (!exact) {
+            atomicAdd(&D.ctl->window_fallbacks, 1);
+            rt_full_scan(D, sgn_a, &q);
+        }
+        result = q;
+    }
+    __syncthreads();
+    return result;
+}
+
+// alpha_i = sum_e a_e rho[row_e] in CSC order (matrix.cpp:273-286), fused with the
+// candidate test; the last block selects q (CHUZC) and runs the BFRT loop
+// (cudaDualSimplex.cpp:484-549).  Phase 1 uses phase1SetRatioTestCandidates.
+template <int BS>
+__global__ void k_pivot_row(Dev D, int mode) {
+    Ctl* c = D.ctl;
+    if (halted(c)) return;
+    const int phase = c->phase;
+    const double sgn_a = (phase == 2) ? (c->is_lower ? -1.0 : 1.0) : (c->f_p > 0 ? -1.0 : 1.0);
+    const int i = blockIdx.x * BS + threadIdx.x;
+    int ncand = 0;
+    if (i < D.n) {
+        const int j = D.nonbasis[i];
+        double acc = 0.0;
+        if (mode & 1) {
+            if (j < D.n) {
+                for (int e = D.cptr[j]; e < D.cptr[j + 1]; ++e) acc += D.cval[e] * D.rho[D.crow[e]];
+            } else {
+                acc += 1.0 * D.rho[j - D.n];
+            }
+            D.alpha[i] = acc;
+        } else {
+            acc = D.alpha[i];
+        }
+        if (mode & 2) {
+            const double a = sgn_a * acc;
+            const double dj = D.d[j];
+            bool cand;
+            if (phase == 2) cand = rt_candidate(a, D.type[j], D.x[j], D.lb[j], D.ub[j]);
+            else cand = (dj >= 0 && a > EPS_A) || (dj <= 0 && a < -EPS_A);
+            double th = CUDART_NAN;
+            if (cand) {
+                ncand = 1;
+                const double tt = dj / a;
+                if (tt < INF_THETA) th = tt;   // NaN and values >= INF are never taken
+            }
+            D.theta_arr[i] = th;
+            D.cand[i] = cand ? 1 : 0;
+        }
+    }
+    ncand = block_sum_int<BS>(ncand);
+    if (!(mode & 2)) return;
+    if (threadIdx.x == 0) D.redi[blockIdx.x] = ncand;
+    if (!last_block(&c->tickets[3])) return;
+    __shared__ int s_tot, s_q;
+    int tot = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += D.redi[b];
+    tot = block_sum_int<BS>(tot);
+    if (threadIdx.x == 0) {
+        s_tot = tot;
+        c->ncand = tot;
+        if (tot == 0) raise_ev(c, phase == 2 ? EV_UNBOUNDED : EV_P1_BLOCK, ST_RATIO);
+        else if (phase == 2) c->unbound_checked = 0;
+    }
+    __syncthreads();
+    if (s_tot == 0) return;
+    // CHUZC part 2 + BFRT
+    double delta = fabs(c->delta);
+    int remaining = s_tot;
+    int q_idx = -1;
+    while (true) {
+        const int qi = rt_select<BS>(D, sgn_a);
+        if (threadIdx.x == 0) s_q = qi;
+        __syncthreads();
+        if (s_q < 0) break;          // nothing takeable (reference: uninitialised q)
+        q_idx = s_q;
+        if (phase != 2) break;
+        const int qv = D.nonbasis[q_idx];
+        if (D.type[qv] != BOXED) break;
+        const double span = (D.ub[qv] - D.lb[qv]) * fabs(sgn_a * D.alpha[q_idx]);
+        if (delta - span <= 0) break;
+        delta -= span;
+        __syncthreads();
+        if (threadIdx.x == 0) D.theta_arr[q_idx] = CUDART_NAN;   // F.erase(q_idx)
+        --remaining;
+        __syncthreads();
+        if (remaining == 0) break;
+    }
+    if (threadIdx.x == 0) {
+        if (q_idx < 0) { c->err = 1; raise_ev(c, EV_ERROR, ST_RATIO); return; }
+        const int qv = D.nonbasis[q_idx];
+        c->q = qv; c->q_idx = q_idx;
+        c->theta = D.d[qv] / D.alpha[q_idx];
+        c->delta_bfrt = (c->is_lower ? -1.0 : 1.0) * delta;
+        if (phase == 1) {
+            // infisibilityCorr(q) (tpp:614-625) on d before the update
+            const unsigned char t = D.type[qv];
+            const double dq = D.d[qv];
+            double corr = 0;
+            if ((t == UPPER || t == FREE) && dq > EPS_D) corr = 1;
+            else if ((t == LOWER || t == FREE) && dq < -EPS_D) corr = -1;
+            c->dz = corr;   // phase 1 reuses dz for the correction term
+        }
+    }
+}
+
+// ================================================================ dual update
+// d_j -= theta alpha_j over the nonbasic slots and the BFRT flip test
+// (cudaDualSimplex.cpp:564-593).  Last block: d_p = -theta, d_q = 0, the ordered
+// flip list, the column change and delta_z, and the dense entering column.
+template <int BS>
+__global__ void k_dual_update(Dev D) {
+    Ctl* c = D.ctl;
+    if (halted(c)) return;
+    const int phase = c->phase;
+    const double theta = c->theta;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    int nf = 0;
+    if (i < D.n) {
+        const int j = D.nonbasis[i];
+        const double dj = D.d[j] - theta * D.alpha[i];
+        D.d[j] = dj;
+        unsigned char fl = 0;
+        if (phase == 2 && D.type[j] == BOXED) {
+            const double x = D.x[j];
+            if (fabs(x - D.lb[j]) < EPS_Z && dj < -EPS_D) fl = 1;
+            else if (fabs(x - D.ub[j]) < EPS_Z && dj > EPS_D) fl = 2;
+        }
+        D.flip[i] = fl;
+        nf = fl ? 1 : 0;
+    }
+    nf = block_sum_int<BS>(nf);
+    if (threadIdx.x == 0) D.redi[blockIdx.x] = nf;
+    if (!last_block(&c->tickets[4])) return;
+    __shared__ int s_nf;
+    int tot = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += D.redi[b];
+    tot = block_sum_int<BS>(tot);
+    if (threadIdx.x == 0) {
+        s_nf = tot;
+        c->nflips = tot;
+        D.d[c->p] = -theta;
+        D.d[c->q] = 0.0;
+        if (phase == 1) c->z_phase1 = c->z_phase1 - theta * c->f_p;
+    }
+    __syncthreads();
+    // entering column a_q as a dense row vector (clear the previous one first)
+    const int pq = c->prev_q;
+    if (pq >= 0) {
+        if (pq < D.n) { for (int e = D.cptr[pq] + threadIdx.x; e < D.cptr[pq + 1]; e += BS) D.aq_dense[D.crow[e]] = 0.0; }
+        else if (threadIdx.x == 0) D.aq_dense[pq - D.n] = 0.0;
+    }
+    __syncthreads();
+    const int q = c->q;
+    if (q < D.n) { for (int e = D.cptr[q] + threadIdx.x; e < D.cptr[q + 1]; e += BS) D.aq_dense[D.crow[e]] = D.cval[e]; }
+    else if (threadIdx.x == 0) D.aq_dense[q - D.n] = 1.0;
+    if (threadIdx.x == 0) { c->prev_q = q; c->nrhs = (s_nf > 0) ? 3 : 2; }
+    if (s_nf == 0) { if (threadIdx.x == 0) c->dz = (phase == 2) ? 0.0 : c->dz; return; }
+    // ---- flips (rare): ordered lists, column change and delta_z in slot order
+    for (int r = threadIdx.x; r < D.m; r += BS) D.cc[r] = 0.0;
+    __syncthreads();
+    __shared__ int nlist;
+    if (threadIdx.x == 0) {
+        double dz = 0.0;
+        int nl = 0;
+        for (int s = 0; s < D.n; ++s) {
+            const unsigned char fl = D.flip[s];
+            if (!fl) continue;
+            const int j = D.nonbasis[s];
+            const double span = D.ub[j] - D.lb[j];
+            if (fl == 1) dz += D.cost[j] * span; else dz -= D.cost[j] * span;
+            D.flip_list[nl++] = (fl == 1) ? j : -(j + 1);
+        }
+        c->dz = dz;
+        nlist = nl;
+    }
+    __syncthreads();
+    // addSparseCol(low, +1) then addSparseCol(up, -1) (matrix.cpp:606-616)
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int u = 0; u < nlist; ++u) {
+            const int code = D.flip_list[u];
+            const bool low = code >= 0;
+            if ((pass == 0) != low) continue;
+            const int j = low ? code : -code - 1;
+            const double span = D.ub[j] - D.lb[j];
+            const double mult = low ? 1.0 : -1.0;
+            if (j < D.n) {
+                for (int e = D.cptr[j] + threadIdx.x; e < D.cptr[j + 1]; e += BS)
+                    D.cc[D.crow[e]] += D.cval[e] * span * mult;
+            } else if (threadIdx.x == 0) {
+                D.cc[j - D.n] += 1.0 * span * mult;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ====================================================================== FTRAN
+// xs_r[j] = sum_t Kinv(j, t) rhs_r[rp_row[t]] for the nr right-hand sides: the
+// t range is split over blockIdx.y chunks; the last chunk block of each j tile
+// adds the partials in chunk order and writes y0 at the structural positions.
+// Tile-wise variant of last_block: arrivals counted per tile over gridDim.y blocks.
+__device__ bool last_in_tile(unsigned* ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.y - 1);
+        if (is_last) *ticket = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+template <int BS>
+__global__ void k_ftran_k2(Dev D, int nr_fixed, int force) {
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
+    const int k = D.k;
+    const int j = blockIdx.x * BS + threadIdx.x;
+    const int t0 = blockIdx.y * D.ftr_chunk;
+    const int t1 = min(k, t0 + D.ftr_chunk);
+    extern __shared__ double sh[];
+    for (int u = threadIdx.x; u < (t1 - t0); u += BS) {
+        const int row = D.rp_row[t0 + u];
+        for (int r = 0; r < nr; ++r) sh[r * D.ftr_chunk + u] = D.frhs[r][row];
+    }
+    __syncthreads();
+    if (j < k) {
+        double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
+        const double* col = D.Kinv + (size_t)t0 * k + j;
+        const int len = t1 - t0;
+        if (nr == 1) {
+            for (int t = 0; t < len; ++t) acc0 += col[(size_t)t * k] * sh[t];
+        } else if (nr == 2) {
+            for (int t = 0; t < len; ++t) {
+                const double kv = col[(size_t)t * k];
+                acc0 += kv * sh[t];
+                acc1 += kv * sh[D.ftr_chunk + t];
+            }
+        } else {
+            for (int t = 0; t < len; ++t) {
+                const double kv = col[(size_t)t * k];
+                acc0 += kv * sh[t];
+                acc1 += kv * sh[D.ftr_chunk + t];
+                acc2 += kv * sh[2 * D.ftr_chunk + t];
+            }
+        }
+        double* part = D.ftr_part + (size_t)blockIdx.y * MAX_FTRAN_RHS * k;
+        part[j] = acc0;
+        if (nr > 1) part[k + j] = acc1;
+        if (nr > 2) part[2 * k + j] = acc2;
+    }
+    if (!last_in_tile(&D.tile_tickets[blockIdx.x])) return;
+    if (j < k) {
+        const int pos = D.s_pos[j];
+        for (int r = 0; r < nr; ++r) {
+            double s = 0.0;
+            for (int ch = 0; ch < (int)gridDim.y; ++ch) s += D.ftr_part[(size_t)ch * MAX_FTRAN_RHS * k + r * k + j];
+            D.y0[r][pos] = s;
+        }
+    }
+}
+
+// Slack rows of B0: y0[slackpos(r)] = rhs[r] - sum_{coupling row r} a * xs.  The
+// last block gathers g_t = y0[p_t] and solves s = Mtri g for the eta chain.
+template <int BS>
+__global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
+    const int r = blockIdx.x * BS + threadIdx.x;
+    if (r < D.m) {
+        const int sp = D.row_slackpos[r];
+        if (sp >= 0) {
+            for (int q = 0; q < nr; ++q) {
+                double s = D.frhs[q][r];
+                for (int e = D.cpl_ptr[r]; e < D.cpl_ptr[r + 1]; ++e)
+                    s -= D.cpl_val[e] * D.y0[q][D.s_pos[D.cpl_col[e]]];
+                D.y0[q][sp] = s;
+            }
+        }
+    }
+    if (!last_block(&c->tickets[5])) return;
+    const int T = c->T;
+    __shared__ double g[MAX_FTRAN_RHS][1024];
+    for (int t = threadIdx.x; t < T; t += BS)
+        for (int q = 0; q < nr; ++q) g[q][t] = D.y0[q][D.eta_pos[t]];
+    __syncthreads();
+    for (int t = threadIdx.x; t < T; t += BS) {
+        const double* Mrow = D.Mtri + (size_t)t * D.cap;
+        for (int q = 0; q < nr; ++q) {
+            double s = 0.0;
+            for (int v = 0; v <= t; ++v) s += Mrow[v] * g[q][v];
+            D.s_eta[q * D.cap + t] = s;
+        }
+    }
+}
+
+// y = y0 + sum_t s_t eta_t (streaming over the eta file); the last block applies
+// the -s_t e_{p_t} terms in eta order and (iteration FTRAN only) the pivot check
+// |alpha_q[p] - alpha_p[q]| > EPS_R (1 + |alpha_q[p]|)  (cudaDualSimplex.cpp:555).
+template <int BS>
+__global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
+    const int T = c->T;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    __shared__ double s[MAX_FTRAN_RHS][256];
+    for (int q = 0; q < nr; ++q)
+        for (int t = threadIdx.x; t < T; t += BS) s[q][t] = D.s_eta[q * D.cap + t];
+    __syncthreads();
+    if (i < D.m) {
+        double a0 = D.y0[0][i], a1 = 0.0, a2 = 0.0;
+        if (nr > 1) a1 = D.y0[1][i];
+        if (nr > 2) a2 = D.y0[2][i];
+        const double* e = D.eta + i;
+        for (int t = 0; t < T; ++t) {
+            const double ev = e[(size_t)t * D.m];
+            a0 += s[0][t] * ev;
+            if (nr > 1) a1 += s[1][t] * ev;
+            if (nr > 2) a2 += s[2][t] * ev;
+        }
+        D.fout[0][i] = a0;
+        if (nr > 1) D.fout[1][i] = a1;
+        if (nr > 2) D.fout[2][i] = a2;
+    }
+    if (!last_block(&c->tickets[6])) return;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < nr; ++q)
+            for (int t = 0; t < T; ++t) {
+                const int pt = D.eta_pos[t];
+                D.fout[q][pt] = D.fout[q][pt] - s[q][t];
+            }
+        if (check) {
+            const double aqp = D.fout[0][c->p_idx];
+            const double apq = D.alpha[c->q_idx];
+            if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
+            else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
+        }
+    }
+}
+
+// ===================================================================== update
+// updateAndChangeBasis (cudaDualSimplex.cpp:254-282) / phase1UpdateAndChangeBasis
+// (:285-309), BFRT x_B correction (:595-617), flips and objective (:618-634).
+template <int BS>
+__global__ void k_update(Dev D, int force) {
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int phase = c->phase;
+    const int p_idx = c->p_idx, T = c->T;
+    const double ap = D.alpha_q[p_idx];
+    const double bp = c->beta_p;
+    const double theta_P = (phase == 2) ? c->delta_bfrt / ap : c->f_p / ap;
+    const int nflips = c->nflips;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    double dzc = 0.0;
+    if (i < D.m) {
+        const int j = D.basis[i];
+        const double aqi = D.alpha_q[i];
+        if (phase == 2) {
+            double xj = D.x[j];
+            if (nflips > 0) { const double dx = D.dxb[i]; xj = xj - dx; dzc = D.cost[j] * dx; }
+            xj = xj - theta_P * aqi;
+            D.x[j] = xj;
+        } else if (i != p_idx) {
+            D.f[i] = D.f[i] - aqi * theta_P;
+        }
+        D.eta[(size_t)T * D.m + i] = (i != p_idx) ? -aqi / ap : 1 / ap;
+        if (i != p_idx) {
+            const double r = aqi / ap;
+            D.beta[i] = D.beta[i] - 2 * aqi / ap * D.tau[i] + (r * r) * bp;
+        }
+    }
+    if (phase == 2 && nflips > 0) {
+        dzc = block_sum<BS>(dzc);
+        if (threadIdx.x == 0) D.red[blockIdx.x] = dzc;
+    }
+    if (!last_block(&c->tickets[7])) return;
+    __shared__ double g[1024];
+    if (threadIdx.x == 0) {
+        const int p = c->p, q = c->q, q_idx = c->q_idx;
+        D.beta[p_idx] = bp / (ap * ap);
+        if (phase == 2) {
+            double dz = c->dz;
+            if (nflips > 0) for (int b = 0; b < (int)gridDim.x; ++b) dz -= D.red[b];
+            c->obj += dz;
+            D.x[q] = D.x[q] + theta_P;
+        } else {
+            D.f[p_idx] = D.f[p_idx] / ap + c->dz;   // + infisibilityCorr
+        }
+        D.basis[p_idx] = q;
+        D.nonbasis[q_idx] = p;
+        D.var_pos[q] = p_idx;
+        D.var_pos[p] = -(q_idx + 1);
+        if (phase == 2 && nflips > 0) {
+            for (int u = 0; u < D.n; ++u) {
+                const int code = D.flip_list[u];
+                if (u >= nflips) break;
+                if (code >= 0) D.x[code] = D.ub[code];
+                else D.x[-code - 1] = D.lb[-code - 1];
+            }
+        }
+        const double theta = c->theta;
+        if (phase == 2) {
+            c->obj += theta * c->delta_bfrt;
+            if (fabs(theta) < EPS_A) c->cycle += 1;
+        } else {
+            c->cycle = (fabs(theta) < EPS_A) ? c->cycle + 1 : 0;
+        }
+        D.eta_pos[T] = p_idx;
+        c->pivots += 1;
+        if (phase == 2 && c->trace_n < c->trace_cap) {
+            const int tn = c->trace_n;
+            D.trace[2 * tn] = p; D.trace[2 * tn + 1] = q;
+            D.trace_d[2 * tn] = theta; D.trace_d[2 * tn + 1] = c->obj;
+        }
+        if (phase == 2) c->trace_n += 1;
+    }
+    // new row of Mtri: G[T][u] = eta_u[p_T] - [p_u == p_T],  M[T][v] = [v == T] + sum_u G[T][u] M[u][v]
+    for (int u = threadIdx.x; u < T; u += BS)
+        g[u] = D.eta[(size_t)u * D.m + p_idx] - (D.eta_pos[u] == p_idx ? 1.0 : 0.0);
+    __syncthreads();
+    for (int v = threadIdx.x; v <= T; v += BS) {
+        double s = (v == T) ? 1.0 : 0.0;
+        for (int u = v; u < T; ++u) s += g[u] * D.Mtri[(size_t)u * D.cap + v];
+        D.Mtri[(size_t)T * D.cap + v] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        c->T = T + 1;
+        if (c->T >= D.cap) raise_ev(c, EV_ETA_FULL, ST_UPDATE);
+    }
+}
+
+// ================================================================ init helpers
+// setPrimalVars (tpp:74-101)
+__global__ void k_set_primal_vars(Dev D) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const int j = D.nonbasis[i];
+    double v;
+    switch (D.type[j]) {
+        case FIXED: v = D.lb[j]; break;
+        case FREE: v = 0; break;
+        case BOXED: v = (D.d[j] > 0) ? D.lb[j] : D.ub[j]; break;
+        case UPPER: v = D.ub[j]; break;
+        default: v = D.lb[j]; break;
+    }
+    D.x[j] = v;
+}
+
+// rhs_i = RHS_i * 1 + sum_e (a_e * x_e) * -1 over nonbasic columns of row i, the
+// slack entry last (dotUpdate UPDATE, matrix.cpp:330-341).
+__global__ void k_xb_rhs(Dev D, double* rhs) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= D.m) return;
+    double s = 0.0 * 1.0;
+    for (int e = D.rptr[r]; e < D.rptr[r + 1]; ++e) {
+        const int cidx = D.rcol[e];
+        const double b = (D.var_pos[cidx] < 0) ? D.x[cidx] : 0.0;
+        s += D.rval[e] * b * -1.0;
+    }
+    const int sl = D.n + r;
+    s += 1.0 * ((D.var_pos[sl] < 0) ? D.x[sl] : 0.0) * -1.0;
+    rhs[r] = s;
+}
+
+__global__ void k_scatter_basic(Dev D, const double* xb, double* dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.m) return;
+    dst[D.basis[i]] = xb[i];
+}
+
+__global__ void k_gather_basic_cost(Dev D, double* cb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.m) return;
+    cb[i] = D.cost[D.basis[i]];
+}
+
+// d_j = sum_e (a_e * y_e) * -1 + c_j for nonbasic j (dotUpdate UPDATE_T, alpha=-1, beta=1).
+__global__ void k_reduced_costs(Dev D, const double* y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D.n) return;
+    const int j = D.nonbasis[i];
+    double acc = 0.0;
+    if (j < D.n) {
+        for (int e = D.cptr[j]; e < D.cptr[j + 1]; ++e) acc += D.cval[e] * y[D.crow[e]] * -1.0;
+    } else {
+        acc += 1.0 * y[j - D.n] * -1.0;
+    }
+    D.d[j] = acc + D.cost[j] * 1.0;
+}
+
+// General BTRAN eta pass for a dense position vector c0:
+//   h_t = eta_t . c0 - c0[p_t]  (one block per t)
+template <int BS>
+__global__ void k_eta_dots(Dev D, const double* c0, double* h) {
+    const int t = blockIdx.x;
+    const double* e = D.eta + (size_t)t * D.m;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < D.m; i += BS) s += e[i] * c0[i];
+    s = block_sum<BS>(s);
+    if (threadIdx.x == 0) h[t] = s - c0[D.eta_pos[t]];
+}
+
+// ybt = c0 + sum_t (Mtri^T h)_t e_{p_t}; marks ybt as dense for the next clear.
+template <int BS>
+__global__ void k_btran_dense_fix(Dev D, const double* c0, const double* h) {
+    __shared__ double dl[1024];
+    const int T = D.ctl->T;
+    for (int i = threadIdx.x; i < D.m; i += BS) D.ybt[i] = c0[i];
+    for (int t = threadIdx.x; t < T; t += BS) {
+        double s = 0.0;
+        for (int v = t; v < T; ++v) s += D.Mtri[(size_t)v * D.cap + t] * h[v];
+        dl[t] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int t = 0; t < T; ++t) { const int pt = D.eta_pos[t]; D.ybt[pt] = D.ybt[pt] + dl[t]; }
+        D.ctl->ybt_n = -1;
+    }
+}
+
+template <int BS>
+__global__ void k_norm2(const double* v, int n, double* out) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += BS) s += v[i] * v[i];
+    s = block_sum<BS>(s);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// obj = c . x over all N (deterministic two-level sum)
+template <int BS>
+__global__ void k_dot_cost_x(Dev D, double* out) {
+    double s = 0.0;
+    for (int j = threadIdx.x; j < D.N; j += BS) s += D.cost[j] * D.x[j];
+    s = block_sum<BS>(s);
+    if (threadIdx.x == 0) *out = s;
+}
+
+// Phase 1 initialisation (tpp:776-795, cudaDualSimplex.cpp:212-226): classify the
+// nonbasic slots, Z, and the column sum of the dual infeasible columns, one block
+// in slot order.
+template <int BS>
+__global__ void k_phase1_init(Dev D, double* cc) {
+    for (int r = threadIdx.x; r < D.m; r += BS) cc[r] = 0.0;
+    __syncthreads();
+    __shared__ double Zs;
+    if (threadIdx.x == 0) Zs = 0.0;
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {   // inf_l (+1) first, then inf_u (-1)
+        for (int i = 0; i < D.n; ++i) {
+            const int j = D.nonbasis[i];
+            const unsigned char t = D.type[j];
+            const double dj = D.d[j];
+            const bool up = (t == UPPER || t == FREE) && dj > EPS_D;
+            const bool lo = !up && (t == LOWER || t == FREE) && dj < -EPS_D;
+            if (!((pass == 0 && lo) || (pass == 1 && up))) continue;
+            const double mult = (pass == 0) ? 1.0 : -1.0;
+            if (threadIdx.x == 0) Zs = (pass == 0) ? Zs + dj : Zs - dj;
+            if (j < D.n) {
+                for (int e = D.cptr[j] + threadIdx.x; e < D.cptr[j + 1]; e += BS) cc[D.crow[e]] += D.cval[e] * mult;
+            } else if (threadIdx.x == 0) {
+                cc[j - D.n] += mult;
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) D.ctl->z_phase1 = Zs;
+}
+
+// counterDualInfeasible into Ctl::p1_dinf (phase 1 pricing needs the count)
+template <int BS>
+__global__ void k_count_dual_inf(Dev D) {
+    Ctl* c = D.ctl;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    int bad = 0;
+    if (i < D.n) { const int j = D.nonbasis[i]; bad = var_dual_bad(D.type[j], D.d[j]) ? 1 : 0; }
+    bad = block_sum_int<BS>(bad);
+    if (threadIdx.x == 0) D.redi[blockIdx.x] = bad;
+    if (!last_block(&c->tickets[8])) return;
+    int tot = 0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += D.redi[b];
+    tot = block_sum_int<BS>(tot);
+    if (threadIdx.x == 0) c->p1_dinf = tot;
+}
+
+// Mtri for an eta file given column by column (one block, rows in order).
+template <int BS>
+__global__ void k_build_mtri(Dev D, int T) {
+    __shared__ double g[1024];
+    for (int t = 0; t < T; ++t) {
+        const int pt = D.eta_pos[t];
+        for (int u = threadIdx.x; u < t; u += BS)
+            g[u] = D.eta[(size_t)u * D.m + pt] - (D.eta_pos[u] == pt ? 1.0 : 0.0);
+        __syncthreads();
+        for (int v = threadIdx.x; v <= t; v += BS) {
+            double s = (v == t) ? 1.0 : 0.0;
+            for (int u = v; u < t; ++u) s += g[u] * D.Mtri[(size_t)u * D.cap + v];
+            D.Mtri[(size_t)t * D.cap + v] = s;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) D.ctl->T = T;
+}
+
+// ================================================================= launchers
+constexpr int BS = 256;
+static inline int nblk(int n) { return (n + BS - 1) / BS; }
+
+#define LAUNCH_OK() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
+
+cudaError_t launch_top(const Dev& D, cudaStream_t s) {
+    k_top<<<1, 32, 0, s>>>(D);
+    k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 0);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_dual_check(const Dev& D, cudaStream_t s) {
+    k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_count_dual_inf(const Dev& D, cudaStream_t s) {
+    k_count_dual_inf<BS><<<nblk(D.n), BS, 0, s>>>(D);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_btran_b0(const Dev& D, double* out, int force, cudaStream_t s) {
+    if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, force);
+    const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
+    k_btran_gemv<BS><<<nbw + nblk(D.m), BS, 0, s>>>(D, out, force);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaStream_t s) {
+    if (D.k > 0) {
+        dim3 g(D.ftr_ntile, D.ftr_nchunk);
+        const size_t sh = (size_t)D.ftr_chunk * MAX_FTRAN_RHS * sizeof(double);
+        k_ftran_k2<BS><<<g, BS, sh, s>>>(D, nr_fixed, force);
+    }
+    k_ftran_assemble<BS><<<nblk(D.m), BS, 0, s>>>(D, nr_fixed, force);
+    k_eta_apply<BS><<<nblk(D.m), BS, 0, s>>>(D, nr_fixed, check, force);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_body(const Dev& D, int from_stage, cudaStream_t s) {
+    if (from_stage <= ST_PRICING) {
+        k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D);
+        cudaError_t e = launch_btran_b0(D, D.rho, 0, s);
+        if (e != cudaSuccess) return e;
+        k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, 3);
+        k_dual_update<BS><<<nblk(D.n), BS, 0, s>>>(D);
+        e = launch_ftran(D, 0, 1, 0, s);
+        if (e != cudaSuccess) return e;
+    }
+    k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 0);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_update_forced(const Dev& D, cudaStream_t s) {
+    k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_iteration(const Dev& D, cudaStream_t s) {
+    cudaError_t e = launch_top(D, s);
+    if (e != cudaSuccess) return e;
+    return launch_body(D, ST_PRICING, s);
+}
+
+cudaError_t launch_set_primal_vars(const Dev& D, cudaStream_t s) {
+    k_set_primal_vars<<<nblk(D.n), BS, 0, s>>>(D);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_xb_rhs(const Dev& D, double* rhs, cudaStream_t s) {
+    k_xb_rhs<<<nblk(D.m), BS, 0, s>>>(D, rhs);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_scatter_basic(const Dev& D, const double* xb, double* dst, cudaStream_t s) {
+    k_scatter_basic<<<nblk(D.m), BS, 0, s>>>(D, xb, dst);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_gather_basic_cost(const Dev& D, double* cb, cudaStream_t s) {
+    k_gather_basic_cost<<<nblk(D.m), BS, 0, s>>>(D, cb);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_reduced_costs(const Dev& D, const double* y, cudaStream_t s) {
+    k_reduced_costs<<<nblk(D.n), BS, 0, s>>>(D, y);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_btran_dense_eta(const Dev& D, const double* c0, double* h, int T, cudaStream_t s) {
+    if (T > 0) k_eta_dots<BS><<<T, BS, 0, s>>>(D, c0, h);
+    k_btran_dense_fix<BS><<<1, BS, 0, s>>>(D, c0, h);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_btran_unit(const Dev& D, int p_idx, cudaStream_t s) {
+    k_btran_unit<BS><<<1, BS, 0, s>>>(D, p_idx);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_norm2(const double* v, int n, double* out, cudaStream_t s) {
+    k_norm2<BS><<<1, BS, 0, s>>>(v, n, out);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_dot_cost_x(const Dev& D, double* out, cudaStream_t s) {
+    k_dot_cost_x<BS><<<1, BS, 0, s>>>(D, out);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_build_mtri(const Dev& D, int T, cudaStream_t s) {
+    k_build_mtri<BS><<<1, BS, 0, s>>>(D, T);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_chuzr_only(const Dev& D, cudaStream_t s) {
+    k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_pivot_row_mode(const Dev& D, int mode, cudaStream_t s) {
+    k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, mode);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_phase1_init(const Dev& D, double* cc, cudaStream_t s) {
+    k_phase1_init<BS><<<1, BS, 0, s>>>(D, cc);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+}  // namespace ds

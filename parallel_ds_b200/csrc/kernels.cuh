@@ -1,0 +1,48 @@
+// Launchers of the engine's kernels (host-callable, stream ordered).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "engine.cuh"
+
+namespace ds {
+
+struct FactorBufs {
+    double* S;        // k*k work array (in-place inverse before the final gather)
+    double* Pan;      // k * NB panel copy
+    double* Wk;       // k * NB working panel
+    int* rowpiv;      // k
+    int* piv_rows;    // k
+    double* Winv;     // NB * NB
+    int* err;         // 1
+    int* s_var;       // k (device copy)
+    int* row_kidx;    // m: row -> K row index or -1
+};
+
+cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s);
+
+cudaError_t launch_top(const Dev& D, cudaStream_t s);
+cudaError_t launch_body(const Dev& D, int from_stage, cudaStream_t s);
+cudaError_t launch_iteration(const Dev& D, cudaStream_t s);
+cudaError_t launch_update_forced(const Dev& D, cudaStream_t s);
+cudaError_t launch_dual_check(const Dev& D, cudaStream_t s);
+cudaError_t launch_count_dual_inf(const Dev& D, cudaStream_t s);
+cudaError_t launch_btran_b0(const Dev& D, double* out, int force, cudaStream_t s);
+cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaStream_t s);
+cudaError_t launch_set_primal_vars(const Dev& D, cudaStream_t s);
+cudaError_t launch_xb_rhs(const Dev& D, double* rhs, cudaStream_t s);
+cudaError_t launch_scatter_basic(const Dev& D, const double* xb, double* dst, cudaStream_t s);
+cudaError_t launch_gather_basic_cost(const Dev& D, double* cb, cudaStream_t s);
+cudaError_t launch_reduced_costs(const Dev& D, const double* y, cudaStream_t s);
+cudaError_t launch_btran_dense_eta(const Dev& D, const double* c0, double* h, int T, cudaStream_t s);
+cudaError_t launch_btran_unit(const Dev& D, int p_idx, cudaStream_t s);
+cudaError_t launch_norm2(const double* v, int n, double* out, cudaStream_t s);
+cudaError_t launch_dot_cost_x(const Dev& D, double* out, cudaStream_t s);
+cudaError_t launch_phase1_init(const Dev& D, double* cc, cudaStream_t s);
+
+// Single-kernel entry points used by the ds_kernel_* C ABI (kernel_api.cu).
+cudaError_t launch_chuzr_only(const Dev& D, cudaStream_t s);
+// mode bit 1: compute alpha from rho (else alpha is given); bit 2: run CHUZC.
+cudaError_t launch_pivot_row_mode(const Dev& D, int mode, cudaStream_t s);
+cudaError_t launch_build_mtri(const Dev& D, int T, cudaStream_t s);
+
+}  // namespace ds

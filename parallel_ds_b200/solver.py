@@ -1,0 +1,245 @@
+"""Host-side mirror of veret-v/parallel_ds's solver interface over the C ABI.
+
+Same names, argument meaning and call order as the reference's mode-1 path
+(src/main.cpp:80-91):
+
+    problem = Problem(bound_type, range_type, costs, lower_range, upper_range,
+                      lower_bound, upper_bound, Matrix(val, row_ptr, col_id, m, n))
+    problem.transformToComputeForm()
+    solver = CudaDualSimplex(problem)
+    solver.initDualSimplex()
+    solver.presolve("minInfeas")
+    solver.solve()
+    solution = problem.getSolution()      # LPsolution(Z, solved, x, message)
+
+Errors follow the reference: an LP with more rows than columns raises
+"Incorrect constraint size" (problem.tpp:230-239); an unknown presolve method
+raises "Unknown phase 1 solver method" (baseDualSimplex.tpp:114-116).
+"""
+import ctypes as C
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+from ._lib import DsError, DsOptions, DsStats, ptr
+
+BOUND_INF = 1e100   # problem.hpp:31
+
+
+class BoundaryType(IntEnum):   # types.hpp:49-57
+    Fixed = 0
+    Free = 1
+    Boxed = 2
+    Upper = 3
+    Lower = 4
+
+
+class Matrix:
+    """CSR matrix, Matrix(elem_csr, row_ptr, col_id, m, n) (matrix.cpp:21-36)."""
+
+    def __init__(self, elem_csr, row_ptr, col_id, m, n):
+        self.val = np.ascontiguousarray(elem_csr, np.float64)
+        self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        self.col_id = np.ascontiguousarray(col_id, np.int32)
+        self.m, self.n = int(m), int(n)
+
+    def getSize(self):
+        return (self.m, self.n)
+
+
+class LPsolution:
+    """LPsolution (LPsolution.hpp:22-42)."""
+
+    def __init__(self, Z=0.0, x=None, solved=False, message=""):
+        self.Z, self.x, self.solved, self.message = Z, x, solved, message
+        self.iterations = 0
+        self.phase2_time = 0.0
+
+    def show(self):
+        print(f"Z = {self.Z}\nsolved = {self.solved}\nmessage = {self.message}")
+
+
+MESSAGES = {1: "optimal solution", 2: "dual unbounded", 3: "dual infeasible",
+            4: "iteration limit", 5: "error", 0: ""}
+
+
+class Problem:
+    """Problem<Matrix, Vector> 8-argument constructor (problem.tpp:143-173)."""
+
+    def __init__(self, bound_type, range_type, costs, lower_range, upper_range, lower_bound,
+                 upper_bound, A):
+        m, n = A.getSize()
+        if m > n:
+            raise RuntimeError("Incorrect constraint size")
+        self.A = A
+        self.bound_type = np.asarray([int(t) for t in bound_type], np.int32)
+        self.range_type = np.asarray([int(t) for t in range_type], np.int32)
+        self.costs = np.asarray(costs, np.float64)
+        self.lower_range = np.asarray(lower_range, np.float64)
+        self.upper_range = np.asarray(upper_range, np.float64)
+        self.lower_bound = np.asarray(lower_bound, np.float64)
+        self.upper_bound = np.asarray(upper_bound, np.float64)
+        self.constraints_size = m
+        self.problem_size = n
+        self.computational = False
+        self._offset = 0.0
+        self.solution = LPsolution()
+
+    @classmethod
+    def from_bounds(cls, A, c, col_lb, col_ub, row_lb, row_ub):
+        """Bound types derived as Problem::readMps does (problem.tpp:350-395)."""
+        def kind(lo, hi):
+            li, hi_ = abs(lo) > BOUND_INF, abs(hi) > BOUND_INF
+            if li and hi_:
+                return BoundaryType.Free
+            if li:
+                return BoundaryType.Upper
+            if hi_:
+                return BoundaryType.Lower
+            return BoundaryType.Fixed if lo == hi else BoundaryType.Boxed
+        bt = [kind(a, b) for a, b in zip(col_lb, col_ub)]
+        rt = [kind(a, b) for a, b in zip(row_lb, row_ub)]
+        return cls(bt, rt, c, row_lb, row_ub, col_lb, col_ub, A)
+
+    def transformToComputeForm(self):
+        """Slack columns are appended inside the engine (problem.tpp:176-226)."""
+        self.computational = True
+
+    def getSolution(self):
+        self.solution.Z -= self._offset
+        return self.solution
+
+
+class CudaDualSimplex:
+    """CudaDualSimplex (cudaDualSimplex.hpp:27-92) backed by libds_b200.so."""
+
+    def __init__(self, problem, refactor_interval=100, max_iterations=2000000, pricing="dse",
+                 strict_reference=False, seed=12345, device=0, learned_margin=0.0, model=None):
+        self.problem = problem
+        self.L = _lib.lib()
+        o = DsOptions()
+        self.L.ds_default_options(C.byref(o))
+        o.refactor_interval = refactor_interval
+        o.max_iterations = max_iterations
+        o.pricing = _lib.PRICING_LEARNED if pricing == "learned" else _lib.PRICING_DSE
+        o.strict_reference = int(bool(strict_reference))
+        o.seed = seed
+        o.device = device
+        o.learned_margin = learned_margin
+        self.opts = o
+        self.h = C.c_void_p()
+        rc = self.L.ds_create(C.byref(o), C.byref(self.h))
+        if rc != 0:
+            raise DsError(rc, "ds_create")
+        self.model = model
+        self.loaded = False
+        self.presolved = False
+
+    def __del__(self):
+        try:
+            if self.h:
+                self.L.ds_destroy(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self.L.ds_last_error(self.h)
+            raise DsError(rc, f"{what}: {msg.decode() if msg else ''}")
+
+    def initDualSimplex(self):
+        p = self.problem
+        A = p.A
+        self._arrs = (A.row_ptr, A.col_id, A.val, p.costs, p.bound_type, p.lower_bound, p.upper_bound,
+                      p.range_type, p.lower_range, p.upper_range)
+        rc = self.L.ds_load_typed(self.h, A.m, A.n, ptr(A.row_ptr, C.c_int), ptr(A.col_id, C.c_int),
+                                  ptr(A.val, C.c_double), ptr(p.costs, C.c_double),
+                                  ptr(p.bound_type, C.c_int), ptr(p.lower_bound, C.c_double),
+                                  ptr(p.upper_bound, C.c_double), ptr(p.range_type, C.c_int),
+                                  ptr(p.lower_range, C.c_double), ptr(p.upper_range, C.c_double))
+        self._check(rc, "ds_load_typed")
+        if self.model is not None:
+            self.model.attach(self)
+        self.loaded = True
+
+    def presolve(self, presolver_method_name="minInfeas"):
+        if presolver_method_name != "minInfeas":
+            raise RuntimeError("Unknown phase 1 solver method")
+        self.presolved = True   # phase 1 runs inside ds_solve, as presolve does before solve()
+
+    def solve(self):
+        if not self.loaded:
+            self.initDualSimplex()
+        rc = self.L.ds_solve(self.h)
+        self._check(rc, "ds_solve")
+        st = self.L.ds_get_status(self.h)
+        n, m = self.problem.A.n, self.problem.A.m
+        x = np.zeros(n)
+        s = np.zeros(m)
+        self.L.ds_get_primal(self.h, ptr(x, C.c_double), ptr(s, C.c_double))
+        sol = self.problem.solution
+        sol.Z = self.L.ds_get_objective(self.h)
+        sol.x = np.concatenate([x, s])
+        sol.solved = st == 1
+        sol.message = MESSAGES.get(st, "")
+        sol.iterations = self.L.ds_get_iterations(self.h)
+        sol.phase2_time = self.stats()["solve_ms"]
+        return sol
+
+    # ---- queries the reference does not expose
+    def status(self):
+        return _lib.STATUS[self.L.ds_get_status(self.h)]
+
+    def dual(self):
+        y = np.zeros(self.problem.A.m)
+        self._check(self.L.ds_get_dual(self.h, ptr(y, C.c_double)), "ds_get_dual")
+        return y
+
+    def reduced_costs(self):
+        d = np.zeros(self.problem.A.n)
+        self._check(self.L.ds_get_reduced_costs(self.h, ptr(d, C.c_double)), "ds_get_reduced_costs")
+        return d
+
+    def basis(self):
+        b = np.zeros(self.problem.A.m, np.int32)
+        self._check(self.L.ds_get_basis(self.h, ptr(b, C.c_int)), "ds_get_basis")
+        return b
+
+    def stats(self):
+        st = DsStats()
+        self.L.ds_get_stats(self.h, C.byref(st))
+        return st.as_dict()
+
+    def set_trace(self, cap):
+        self._check(self.L.ds_set_trace(self.h, int(cap)), "ds_set_trace")
+
+    def trace(self):
+        cap = 1 << 22
+        cnt = C.c_int(0)
+        self.L.ds_get_trace(self.h, None, None, None, None, C.byref(cnt))
+        k = cnt.value
+        p = np.zeros(k, np.int32); q = np.zeros(k, np.int32)
+        th = np.zeros(k); ob = np.zeros(k)
+        self.L.ds_get_trace(self.h, ptr(p, C.c_int), ptr(q, C.c_int), ptr(th, C.c_double),
+                            ptr(ob, C.c_double), C.byref(cnt))
+        del cap
+        return dict(p=p, q=q, theta=th, obj=ob)
+
+
+def solve_lp(lp, **opts):
+    """Solve a generated LP dict (lp.generate) and return a result dict."""
+    from .lp import typed
+    t = typed(lp)
+    A = Matrix(t["val"], t["row_ptr"], t["col_idx"], t["m"], t["n"])
+    prob = Problem(t["col_type"], t["row_type"], t["c"], t["row_lb"], t["row_ub"], t["col_lb"],
+                   t["col_ub"], A)
+    prob.transformToComputeForm()
+    s = CudaDualSimplex(prob, **opts)
+    s.initDualSimplex()
+    s.presolve("minInfeas")
+    sol = s.solve()
+    out = dict(status=s.status(), objective=sol.Z, x=sol.x, iterations=sol.iterations,
+               stats=s.stats(), dual=s.dual(), reduced_costs=s.reduced_costs(), basis=s.basis())
+    return out
