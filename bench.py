@@ -1,0 +1,355 @@
+#!/usr/bin/env python
+"""Benchmark: time-to-optimal and iterations/s of the B200 dual simplex.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload learned|plain_small|plain_large] [--pricing dse|learned]
+
+One step = one complete solve (phase 1 + phase 2 to optimality) of one seeded
+LP from the workload's distribution (default: m=2000, n=4000, 1% N(0,1)
+entries, b = A x0 + U[0.1,1], c ~ U[0,1]; held-out seeds 2000+).  Each rank
+solves its own seeds (independent LPs: replicas, weak scaling, no collective in
+the solve).  `value` is total simplex iterations / the max over ranks of the
+summed per-step device time (CUDA events on the solver's stream) with every LP
+already resident in HBM; `e2e` is the same through the public C ABI from pinned
+host buffers (ds_load_typed -> ds_solve -> ds_get_primal / ds_get_dual).
+Rank 0 prints one JSON line.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-optimal & iters/s: learned vs plain GPU dual simplex, obj rel-err ≤1e-9"
+WORKLOADS = {
+    "learned": dict(desc="LP m=2000 n=4000 density 1% N(0,1), A x <= b, x >= 0", m=2000, n=4000),
+    "plain_small": dict(desc="LP m=200 n=400 density 5% N(0,1), A x <= b, x >= 0", m=200, n=400),
+    "plain_large": dict(desc="LP m=50000 n=100000 8 nnz/col N(0,1), A x <= b, x >= 0", m=50000, n=100000),
+}
+
+
+def gen(workload, seed):
+    from parallel_ds_b200 import lp as L
+    return {"learned": L.learned, "plain_small": L.plain_small, "plain_large": L.plain_large}[workload](seed)
+
+
+def lp_bytes(t):
+    return sum(int(t[k].nbytes) for k in ("row_ptr", "col_idx", "val", "c", "col_type", "col_lb", "col_ub",
+                                          "row_type", "row_lb", "row_ub"))
+
+
+class Clocks(threading.Thread):
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        super().__init__(daemon=True)
+        self.dev, self.rows, self.stop_ev, self.proc = dev, [], threading.Event(), None
+
+    def run(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            for line in self.proc.stdout:
+                self.rows.append([x.strip() for x in line.split(",")])
+                if self.stop_ev.is_set():
+                    break
+        except Exception:
+            pass
+
+    def stop(self):
+        self.stop_ev.set()
+        if self.proc:
+            self.proc.terminate()
+        self.join(timeout=3)
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def pinned_copy(t):
+    """The typed LP's arrays in page-locked host memory (torch allocator)."""
+    import numpy as np
+    import torch
+    out = {}
+    for k, v in t.items():
+        if isinstance(v, np.ndarray):
+            buf = torch.empty(v.shape, dtype=torch.from_numpy(v[:0].copy()).dtype, pin_memory=True)
+            buf.numpy()[...] = v
+            out[k] = buf.numpy()
+        else:
+            out[k] = v
+    return out
+
+
+def our_arm(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from parallel_ds_b200 import _lib
+    from parallel_ds_b200 import lp as L
+    from parallel_ds_b200._lib import DsOptions, DsStats, ptr
+
+    torch.cuda.set_device(local_rank)
+    lib = _lib.lib()
+    stream = torch.cuda.Stream()
+    o = DsOptions()
+    lib.ds_default_options(C.byref(o))
+    o.device = local_rank
+    o.stream = C.c_void_p(stream.cuda_stream)
+    o.pricing = _lib.PRICING_LEARNED if args.pricing == "learned" else _lib.PRICING_DSE
+
+    def new_handle():
+        h = C.c_void_p()
+        assert lib.ds_create(C.byref(o), C.byref(h)) == 0
+        return h
+
+    def load(h, t):
+        rc = lib.ds_load_typed(h, t["m"], t["n"], ptr(t["row_ptr"], C.c_int), ptr(t["col_idx"], C.c_int),
+                               ptr(t["val"], C.c_double), ptr(t["c"], C.c_double), ptr(t["col_type"], C.c_int),
+                               ptr(t["col_lb"], C.c_double), ptr(t["col_ub"], C.c_double),
+                               ptr(t["row_type"], C.c_int), ptr(t["row_lb"], C.c_double),
+                               ptr(t["row_ub"], C.c_double))
+        assert rc == 0, lib.ds_last_error(h)
+
+    def stats(h):
+        s = DsStats()
+        lib.ds_get_stats(h, C.byref(s))
+        return s
+
+    K, W = args.steps, args.warmup
+    seeds = [2000 + rank * K + s for s in range(K)]
+    wseeds = [1000 + rank * W + s for s in range(W)]
+    lps = [pinned_copy(L.typed(gen(args.workload, s))) for s in seeds]
+    wlps = [pinned_copy(L.typed(gen(args.workload, s))) for s in wseeds]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # warm-up (untimed)
+    for t in wlps:
+        h = new_handle(); load(h, t)
+        assert lib.ds_solve(h) == 0, lib.ds_last_error(h)
+        lib.ds_destroy(h)
+
+    # ---- value: LPs resident in HBM, K solves
+    handles = []
+    for t in lps:
+        h = new_handle(); load(h, t); handles.append(h)
+    torch.cuda.synchronize()
+    clk = Clocks(local_rank) if rank == 0 else None
+    if clk:
+        clk.start(); time.sleep(0.6)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    barrier(); torch.cuda.synchronize()
+    launches0 = lib.ds_kernel_launch_count()
+    iters, statuses = 0, []
+    with torch.cuda.stream(stream):
+        for s, h in enumerate(handles):
+            flush.fill_(float(s))                 # evict the previous step's working set from L2
+            ev[s][0].record(stream)
+            rc = lib.ds_solve(h)
+            ev[s][1].record(stream)
+            assert rc == 0, lib.ds_last_error(h)
+            iters += stats(h).iterations
+            statuses.append(lib.ds_get_status(h))
+    torch.cuda.synchronize(); barrier()
+    launches = lib.ds_kernel_launch_count() - launches0
+    clocks = clk.stop() if clk else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_ms = sum(step_ms)
+    iter_counts = [stats(h).iterations for h in handles]
+    objs = [lib.ds_get_objective(h) for h in handles]
+    solve_stats = [stats(h) for h in handles]
+
+    # ---- e2e: public API from pinned host buffers, H2D + D2H inside the timed region
+    h2d = sum(lp_bytes(t) for t in lps) // K
+    d2h = 8 * (lps[0]["n"] + lps[0]["m"]) + 8 * lps[0]["m"]
+    xs = [np.zeros(t["n"]) for t in lps]
+    ys = [np.zeros(t["m"]) for t in lps]
+    eh = new_handle()
+    barrier(); torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    ee = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    ee[0].record(stream)
+    for s, t in enumerate(lps):
+        load(eh, t)
+        assert lib.ds_solve(eh) == 0
+        lib.ds_get_primal(eh, ptr(xs[s], C.c_double), None)
+        lib.ds_get_dual(eh, ptr(ys[s], C.c_double))
+    ee[1].record(stream)
+    torch.cuda.synchronize(); barrier()
+    e_wall_ms = (time.perf_counter() - e0) * 1e3
+    e_ms = ee[0].elapsed_time(ee[1])
+    lib.ds_destroy(eh)
+
+    # ---- roofline of the dominant kernel (replayed on the final state of step 0)
+    roof = None
+    roof = profile_roofline(lib, handles[0])
+
+    for h in handles:
+        lib.ds_destroy(h)
+
+    # reduce over ranks: max time, summed iterations
+    if world > 1:
+        tt = torch.tensor([t_ms, e_ms, e_wall_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        it = torch.tensor([iters], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(it, op=torch.distributed.ReduceOp.SUM)
+        t_ms, e_ms, e_wall_ms = [float(v) for v in tt.tolist()]
+        iters_all = int(it.item())
+    else:
+        iters_all = iters
+    if rank != 0:
+        return None
+    e_ms_used = max(e_ms, e_wall_ms)
+    res = {
+        "metric": METRIC,
+        "value": iters_all / (t_ms / 1e3),
+        "unit": "iters/s",
+        "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t_ms / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: seeded generator, N(0,1) entries, x0~U[0,1], b=A x0+U[0.1,1], c~U[0,1]",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": args.pricing,
+                   "seeds_rank0": seeds, "refactor_interval": 100, "parallelism": f"replicas x{world}",
+                   "l2": "256 MB buffer written between steps (flush); each step is a full solve",
+                   "step": "one complete solve to optimality"},
+        "time_to_optimal_ms": step_ms,
+        "iterations": iter_counts,
+        "objectives": objs,
+        "statuses": [_status(s) for s in statuses],
+        "refactor_ms": [s.refactor_ms for s in solve_stats],
+        "e2e": {"value": iters_all / (e_ms_used / 1e3), "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms_used / K},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if roof:
+        res["roofline"] = roof
+    return res
+
+
+def _status(code):
+    from parallel_ds_b200._lib import STATUS
+    return STATUS.get(code, str(code))
+
+
+def profile_roofline(lib, h):
+    """Per-kernel device times measured by the engine's replay profiler."""
+    import json as _j
+    buf = C.create_string_buffer(1 << 16)
+    if lib.ds_profile_solve(h, buf, len(buf)) != 0:
+        return None
+    prof = _j.loads(buf.value.decode())
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    top = max(prof["kernels"], key=lambda k: k["share"])
+    achieved = top["bytes"] / (top["avg_us"] * 1e-6) / 1e9
+    return {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_source": "measured" if peaks else "fallback",
+            "kernels": prof["kernels"]}
+
+
+def cpu_sample(workload, seconds=15.0, threads=1):
+    """The oracle (CPU port of the reference) on a bounded sample of the workload."""
+    from oracle import pyoracle as po
+    from parallel_ds_b200 import lp as L
+    t = L.typed(gen(workload, 2000))
+    # size the iteration cap from a short probe so the sample takes ~`seconds`
+    t0 = time.perf_counter()
+    r = po.solve_typed(t, max_iterations=200)
+    dt = time.perf_counter() - t0
+    cap = int(max(200, min(200 * seconds / max(dt, 1e-3) * 0.6, 1e6)))
+    t0 = time.perf_counter()
+    r = po.solve_typed(t, max_iterations=cap)
+    dt = time.perf_counter() - t0
+    return {"value": r["iterations"] / dt, "unit": "iters/s", "cores": threads, "kind": "port",
+            "sample": f"oracle on seed 2000, first {r['iterations']} iterations ({r['status']}), {dt:.1f} s"}
+
+
+def reference_arm(args):
+    """The reference's CPU algorithm (oracle port) on the host cores, one LP per thread."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import pyoracle as po
+    from parallel_ds_b200 import lp as L
+    cores = os.cpu_count() or 1
+    K, W = args.steps, args.warmup
+    # bounded sample per step: iteration cap sized so the run ends in a few minutes
+    cap = {"plain_small": 10**6, "learned": 4000, "plain_large": 300}[args.workload]
+    lps = [L.typed(gen(args.workload, 2000 + s)) for s in range(K)]
+    for s in range(min(W, 1)):
+        po.solve_typed(L.typed(gen(args.workload, 1000 + s)), max_iterations=min(cap, 200))
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=min(cores, K)) as ex:
+        rs = list(ex.map(lambda t: po.solve_typed(t, max_iterations=cap), lps))
+    dt = time.perf_counter() - t0
+    iters = sum(r["iterations"] for r in rs)
+    v = iters / dt
+    return {
+        "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 0, "steps": K, "warmup": W,
+        "ms_per_step": dt * 1e3 / K * min(cores, K), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic: same seeded LPs as the GPU arm",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": "dse",
+                   "sample": f"first {cap} iterations of each step's LP"},
+        "cpu_baseline": {"value": v, "unit": "iters/s", "cores": min(cores, K), "kind": "port",
+                         "sample": f"{K} LPs (seeds 2000..{2000 + K - 1}), <= {cap} iterations each, "
+                                   f"one LP per host thread"},
+        "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "statuses": [r["status"] for r in rs], "iterations": [r["iterations"] for r in rs],
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="learned", choices=sorted(WORKLOADS))
+    ap.add_argument("--pricing", default="dse", choices=["dse", "learned"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args)))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    res = our_arm(args, rank, world, local_rank)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_sample(args.workload)
+        print(json.dumps(res))
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -140,6 +140,24 @@ int ds_set_trace(ds_solver* s, int cap);
 int ds_get_trace(const ds_solver* s, int* p, int* q, double* theta, double* obj, int* count);
 
 
+/* Factorise the basis given as m variable indices (structurals 0..n-1, slacks
+ * n..n+m-1) and apply B^-1 (transpose = 0: rhs by rows -> out by basis
+ * positions) or B^-T (transpose = 1: positions -> rows) to nrhs vectors of m
+ * doubles stored one after another.  Replaces the reference's
+ * CudaDualSimplex::solveLinSys after reFactorize (cudaDualSimplex.cpp:105-151,
+ * 229-238); the loaded LP supplies A. */
+int ds_basis_solve(ds_solver* s, const int* basis, const double* rhs, double* out, int nrhs, int transpose);
+
+/* Kernels launched by this library in this process so far (graph replays
+ * counted per kernel node).  No reference counterpart. */
+long long ds_kernel_launch_count(void);
+
+/* Re-solve the loaded LP with every iteration kernel bracketed by CUDA events
+ * (one iteration per synchronisation) and write a JSON summary: per kernel its
+ * launches, total and mean device time, algorithmic bytes per launch and share.
+ * Stands in for the reference's TimeProfiler report (timeProfiler.cpp:108-148). */
+int ds_profile_solve(ds_solver* s, char* json, int len);
+
 /* ---- kernel-level entry points (run one device kernel on host vectors) ----
  * For index-selection parity against the reference on identical inputs. */
 

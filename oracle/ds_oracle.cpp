@@ -557,7 +557,11 @@ struct Oracle {
             if (iteration % NEED_RESTART == 0 && !dual_feasible()) {
                 refactor(); phase1(); dual_simplex_init(); ++restarts;
             }
-            if (!perturbed && cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); }
+            if (!perturbed && cycle > MAX_CYCLE) {
+                perturb(); refactor(); dual_simplex_init();
+                // guard: the perturbed reduced costs may be dual infeasible
+                if (!opt.strict_reference && !dual_feasible()) { refactor(); phase1(); dual_simplex_init(); ++restarts; }
+            }
             if (primal_feasible()) { status = ST_OPTIMAL; break; }
             // DSEPricing (tpp:470-501); blocked set is always empty in phase 2
             double maxw = 0, delta = 0; int p = -1, p_idx = -1; bool is_lower = false;

@@ -113,6 +113,13 @@ struct Engine {
     std::vector<int> basis_out;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evr0 = nullptr, evr1 = nullptr;
     MlpModel* mlp = nullptr;    // learned pricing (not owned)
+    long long graph_nodes = 0;  // kernel nodes in the iteration graph
+    long long nnz_S = 0, nnz_cpl = 0;   // structural nonzeros in the basis / coupling rows
+    // per-kernel profiling (ds_profile_solve)
+    bool prof = false;
+    double prof_us[S_NSTEPS] = {}, prof_bytes[S_NSTEPS] = {};
+    long long prof_n[S_NSTEPS] = {};
+    cudaEvent_t pev[2 * S_NSTEPS] = {};
 
     // --------------------------------------------------------------- setup
     explicit Engine(const ds_options& o) : opt(o) {
@@ -130,12 +137,13 @@ struct Engine {
         if (ev1) cudaEventDestroy(ev1);
         if (evr0) cudaEventDestroy(evr0);
         if (evr1) cudaEventDestroy(evr1);
+        for (auto& e : pev) if (e) cudaEventDestroy(e);
         if (own_stream && stream) cudaStreamDestroy(stream);
     }
 
     template <typename T>
     void up(DBuf<T>& b, const std::vector<T>& v) {
-        b.alloc(v.size());
+        b.ensure(v.size());
         if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     }
 
@@ -181,25 +189,25 @@ struct Engine {
         up(d_cptr, h_cptr); up(d_crow, h_crow); up(d_cval, h_cval);
         up(d_lb, h_lb); up(d_ub, h_ub); up(d_cost, h_cost); up(d_type, h_type);
         // iteration state
-        d_x.alloc(N); d_d.alloc(N); d_beta.alloc(m); d_f.alloc(m);
-        d_basis.alloc(m); d_nonbasis.alloc(n); d_var_pos.alloc(N); d_blocked.alloc(N);
-        d_s_pos.alloc(m); d_s_var.alloc(m); d_rp_row.alloc(m); d_pos_kidx.alloc(m);
-        d_row_slackpos.alloc(m); d_row_kidx.alloc(m);
-        d_cpl_ptr.alloc(m + 1); d_cpl_col.alloc(std::max(nnz, 1)); d_cpl_val.alloc(std::max(nnz, 1));
+        d_x.ensure(N); d_d.ensure(N); d_beta.ensure(m); d_f.ensure(m);
+        d_basis.ensure(m); d_nonbasis.ensure(n); d_var_pos.ensure(N); d_blocked.ensure(N);
+        d_s_pos.ensure(m); d_s_var.ensure(m); d_rp_row.ensure(m); d_pos_kidx.ensure(m);
+        d_row_slackpos.ensure(m); d_row_kidx.ensure(m);
+        d_cpl_ptr.ensure(m + 1); d_cpl_col.ensure(std::max(nnz, 1)); d_cpl_val.ensure(std::max(nnz, 1));
         cap = std::min(std::max(opt.refactor_interval, 1), 240) + 5;
-        d_eta.alloc((size_t)cap * m); d_Mtri.alloc((size_t)cap * cap); d_eta_pos.alloc(cap); d_ybt_pos.alloc(cap + 1);
-        d_rho.alloc(m); d_alpha.alloc(n); d_theta.alloc(n); d_cand.alloc(n); d_ybt.alloc(m);
-        d_btr_rhs.alloc(m); d_aq.alloc(m); d_cc.alloc(m); d_alpha_q.alloc(m); d_tau.alloc(m); d_dxb.alloc(m);
-        for (auto& b : d_y0) b.alloc(m);
-        d_seta.alloc((size_t)MAX_FTRAN_RHS * cap);
+        d_eta.ensure((size_t)cap * m); d_Mtri.ensure((size_t)cap * cap); d_eta_pos.ensure(cap); d_ybt_pos.ensure(cap + 1);
+        d_rho.ensure(m); d_alpha.ensure(n); d_theta.ensure(n); d_cand.ensure(n); d_ybt.ensure(m);
+        d_btr_rhs.ensure(m); d_aq.ensure(m); d_cc.ensure(m); d_alpha_q.ensure(m); d_tau.ensure(m); d_dxb.ensure(m);
+        for (auto& b : d_y0) b.ensure(m);
+        d_seta.ensure((size_t)MAX_FTRAN_RHS * cap);
         const int nb = std::max((m + 255) / 256, (n + 255) / 256) + 8;
-        d_red.alloc(2 * nb); d_redi.alloc(2 * nb);
-        d_flip.alloc(n); d_flip_list.alloc(n);
-        d_tmp_rows.alloc(m); d_tmp_rows2.alloc(m); d_tmp_pos.alloc(m); d_tmp_pos2.alloc(m); d_h.alloc(cap);
-        d_ctl.alloc(1);
-        d_Winv.alloc(16 * 16); d_ferr.alloc(1);
-        d_trace.alloc(2); d_trace_d.alloc(2);
-        d_feat.alloc((size_t)m * 12); d_score.alloc(m);
+        d_red.ensure(2 * nb); d_redi.ensure(2 * nb);
+        d_flip.ensure(n); d_flip_list.ensure(n);
+        d_tmp_rows.ensure(m); d_tmp_rows2.ensure(m); d_tmp_pos.ensure(m); d_tmp_pos2.ensure(m); d_h.ensure(cap);
+        d_ctl.ensure(1);
+        d_Winv.ensure(16 * 16); d_ferr.ensure(1);
+        d_trace.ensure(2); d_trace_d.ensure(2);
+        d_feat.ensure((size_t)m * 12); d_score.ensure(m);
         std::vector<int> rc(m);
         for (int i = 0; i < m; ++i) rc[i] = h_rptr[i + 1] - h_rptr[i];
         up(d_row_cnt, rc);
@@ -267,6 +275,8 @@ struct Engine {
         for (int r = 0; r < m; ++r) if (row_slackpos[r] < 0) { row_kidx[r] = (int)rp_row.size(); rp_row.push_back(r); }
         k = (int)s_pos.size();
         if ((int)rp_row.size() != k) throw CudaError("basis is structurally singular", DS_ERR_NUMERIC);
+        nnz_S = 0;
+        for (int v : s_var) nnz_S += h_cptr[v + 1] - h_cptr[v];
         // coupling rows: A[r, S] for rows r whose slack is basic, CSR column order
         std::vector<int> cptr(m + 1, 0), ccol; std::vector<double> cval;
         for (int r = 0; r < m; ++r) {
@@ -282,6 +292,7 @@ struct Engine {
         };
         put(d_s_pos, s_pos); put(d_s_var, s_var); put(d_rp_row, rp_row);
         put(d_row_slackpos, row_slackpos); put(d_pos_kidx, pos_kidx); put(d_row_kidx, row_kidx);
+        nnz_cpl = (long long)ccol.size();
         put(d_cpl_ptr, cptr); put(d_cpl_col, ccol);
         if (!cval.empty()) CK(cudaMemcpyAsync(d_cpl_val.p, cval.data(), cval.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
         const size_t kk = (size_t)std::max(k, 1) * std::max(k, 1);
@@ -309,7 +320,38 @@ struct Engine {
         CK(cudaStreamSynchronize(stream));
         float ms = 0; cudaEventElapsedTime(&ms, evr0, evr1);
         st.refactor_ms += ms;
-        if (k > 0 && ferr) throw CudaError("singular basis in refactorisation", DS_ERR_NUMERIC);
+        if (k > 0 && ferr) {
+            // diagnostics: duplicate basic variables, K columns without an R' entry
+            std::vector<int> seen(N, 0);
+            int dups = 0, empty_cols = 0;
+            for (int v : basis) if (seen[v]++) ++dups;
+            for (int j = 0; j < k; ++j) {
+                bool any = false;
+                for (int e = h_cptr[s_var[j]]; e < h_cptr[s_var[j] + 1]; ++e) any |= row_kidx[h_crow[e]] >= 0;
+                if (!any) ++empty_cols;
+            }
+            char msg[256];
+            snprintf(msg, sizeof(msg), "singular basis in refactorisation (iteration %d, k %d, pivot column %d, "
+                     "duplicate basics %d, empty K columns %d)", hc->iteration, k, ferr - 1, dups, empty_cols);
+            throw CudaError(msg, DS_ERR_NUMERIC);
+        }
+        if (opt.verbose >= 3 && k > 0) {
+            // debug: || Kinv K - I ||_max on the host
+            std::vector<double> Ki((size_t)k * k), Kd((size_t)k * k, 0.0);
+            CK(cudaMemcpyAsync(Ki.data(), d_Kinv.p, sizeof(double) * k * k, cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            for (int j = 0; j < k; ++j)
+                for (int e = h_cptr[s_var[j]]; e < h_cptr[s_var[j] + 1]; ++e)
+                    if (row_kidx[h_crow[e]] >= 0) Kd[(size_t)row_kidx[h_crow[e]] + (size_t)j * k] = h_cval[e];
+            double worst = 0;
+            for (int i = 0; i < k; ++i)
+                for (int j = 0; j < k; ++j) {
+                    double s2 = 0;
+                    for (int t = 0; t < k; ++t) s2 += Ki[(size_t)i + (size_t)t * k] * Kd[(size_t)t + (size_t)j * k];
+                    worst = std::max(worst, std::fabs(s2 - (i == j ? 1.0 : 0.0)));
+                }
+            fprintf(stderr, "[ds-check] refactor it %d k %d |Kinv K - I| %.3e (%.2f ms)\n", hc->iteration, k, worst, ms);
+        }
         hc->T = 0;
         hc->k = k;
         push();
@@ -326,9 +368,14 @@ struct Engine {
         if (gexec) return;
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        set_launch_counting(false);
         cudaError_t le = launch_iteration(D, stream);
+        set_launch_counting(true);
         cudaError_t ce = cudaStreamEndCapture(stream, &g);
         CK(le); CK(ce);
+        size_t nn = 0;
+        CK(cudaGraphGetNodes(g, nullptr, &nn));
+        graph_nodes = (long long)nn;
         CK(cudaGraphInstantiate(&gexec, g, 0));
         cudaGraphDestroy(g);
     }
@@ -511,7 +558,144 @@ struct Engine {
 
     // -------------------------------------------------------------- phase 2
     // Launch graph iterations until an event is raised.
+    // Algorithmic bytes moved by one launch of each iteration kernel (FP64 = 8 B,
+    // int32 = 4 B), with T the eta count at the start of the iteration.
+    double step_bytes(int st, int T, int nrhs, bool dual_check) const {
+        const double M = m, Nn = n, K = k, Tt = T, R = nrhs;
+        switch (st) {
+            case S_TOP: return 16;
+            case S_DUALCHECK: return dual_check ? 13 * Nn : 0;
+            case S_CHUZR: return 37 * M + 8 * Tt + 4 * Tt * Tt;
+            case S_BTRAN_RHS: return 24.0 * nnz_S + 20 * K;
+            case S_BTRAN_GEMV: return 8 * K * K + 8 * K + 12 * M;
+            case S_PIVOT_ROW: return 12.0 * ((double)h_rptr[m] - nnz_S) + 8 * K + 4 * Nn + 8 * (Nn - K) + 8 * M + 50 * Nn;
+            case S_DUAL_UPDATE: return 30 * Nn;
+            case S_FTRAN_K: return 8 * K * K + 16 * R * K + 8 * R * K * D.ftr_nchunk;
+            case S_FTRAN_ASM: return 20.0 * nnz_cpl + (M - K) * (4 + 16 * R) + 8 * R * Tt;
+            case S_ETA_APPLY: return 8 * Tt * M + 16 * R * M;
+            case S_UPDATE: return 60 * M + 8 * Tt + 4 * Tt * Tt;
+        }
+        return 0;
+    }
+
+    // Debug self-check (verbose >= 3): residuals of this iteration's solves
+    // against the basis it started from, computed on the host in O(nnz).
+    std::vector<int> dbg_basis;
+    void debug_check_iteration() {
+        std::vector<double> aq(m), rho(m), tau(m), x(N);
+        CK(cudaMemcpyAsync(aq.data(), d_alpha_q.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(rho.data(), d_rho.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(tau.data(), d_tau.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(x.data(), d_x.p, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        auto col_axpy = [&](int v, double a, std::vector<double>& out) {
+            if (v < n) { for (int e = h_cptr[v]; e < h_cptr[v + 1]; ++e) out[h_crow[e]] += a * h_cval[e]; }
+            else out[v - n] += a;
+        };
+        auto col_dot = [&](int v, const std::vector<double>& y) {
+            double s = 0;
+            if (v < n) { for (int e = h_cptr[v]; e < h_cptr[v + 1]; ++e) s += h_cval[e] * y[h_crow[e]]; }
+            else s = y[v - n];
+            return s;
+        };
+        const std::vector<int>& B = dbg_basis;
+        std::vector<double> r1(m, 0.0), r3(m, 0.0);
+        for (int i = 0; i < m; ++i) { col_axpy(B[i], aq[i], r1); col_axpy(B[i], tau[i], r3); }
+        col_axpy(hc->q, -1.0, r1);
+        double e1 = 0, e2 = 0, e3 = 0, nr = 0;
+        for (int r = 0; r < m; ++r) { e1 = std::max(e1, std::fabs(r1[r])); e3 = std::max(e3, std::fabs(r3[r] - rho[r])); nr = std::max(nr, std::fabs(rho[r])); }
+        for (int i = 0; i < m; ++i) e2 = std::max(e2, std::fabs(col_dot(B[i], rho) - (i == hc->p_idx ? 1.0 : 0.0)));
+        // primal residual with the new basis: A x + s = 0 over all columns
+        std::vector<double> rp(m, 0.0);
+        for (int j = 0; j < N; ++j) if (x[j] != 0.0) col_axpy(j, x[j], rp);
+        double e4 = 0; for (double v : rp) e4 = std::max(e4, std::fabs(v));
+        if (e1 > 1e-8 || e2 > 1e-8 || e3 > 1e-8 * (1 + nr) || e4 > 1e-7)
+            fprintf(stderr, "[ds-check] it %d k %d T %d p_idx %d q %d |B aq - a_q| %.3e |B^T rho - e_p| %.3e |B tau - rho| %.3e |Ax+s| %.3e\n",
+                    hc->iteration, k, hc->T, hc->p_idx, hc->q, e1, e2, e3, e4);
+    }
+
+    // Debug: does B0 + the eta file still represent the current basis?  FTRAN and
+    // BTRAN of random vectors checked against the basis read back from the device.
+    void debug_check_representation(const char* where) {
+        std::vector<int> B(m);
+        CK(cudaMemcpyAsync(B.data(), d_basis.p, sizeof(int) * m, cudaMemcpyDeviceToHost, stream));
+        std::vector<double> r(m), y(m), c(m), z(m);
+        uint64_t st2 = 0x9E3779B97F4A7C15ull ^ (uint64_t)hc->iteration;
+        for (int i = 0; i < m; ++i) { st2 = st2 * 6364136223846793005ull + 1442695040888963407ull; r[i] = (double)(st2 >> 11) * 0x1.0p-53 - 0.5; c[i] = r[(i * 7) % m]; }
+        CK(cudaMemcpyAsync(d_tmp_rows.p, r.data(), sizeof(double) * m, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_tmp_pos.p, c.data(), sizeof(double) * m, cudaMemcpyHostToDevice, stream));
+        ftran1(d_tmp_rows.p, d_tmp_pos2.p);
+        btran_dense(d_tmp_pos.p, d_tmp_rows2.p);
+        CK(cudaMemcpyAsync(y.data(), d_tmp_pos2.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(z.data(), d_tmp_rows2.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        std::vector<double> By(m, 0.0);
+        double e1 = 0, e2 = 0;
+        for (int i = 0; i < m; ++i) {
+            const int v = B[i];
+            if (v < n) { for (int e = h_cptr[v]; e < h_cptr[v + 1]; ++e) By[h_crow[e]] += h_cval[e] * y[i]; }
+            else By[v - n] += y[i];
+            double d2 = 0;
+            if (v < n) { for (int e = h_cptr[v]; e < h_cptr[v + 1]; ++e) d2 += h_cval[e] * z[h_crow[e]]; }
+            else d2 = z[v - n];
+            e2 = std::max(e2, std::fabs(d2 - c[i]));
+        }
+        for (int i = 0; i < m; ++i) e1 = std::max(e1, std::fabs(By[i] - r[i]));
+        if (e1 > 1e-9 || e2 > 1e-9)
+            fprintf(stderr, "[ds-rep] %s it %d k %d T %d |B FTRAN(r) - r| %.3e |B^T BTRAN(c) - c| %.3e\n",
+                    where, hc->iteration, k, hc->T, e1, e2);
+    }
+
+    void debug_check_x(const char* where) {
+        std::vector<double> x(N);
+        CK(cudaMemcpyAsync(x.data(), d_x.p, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        std::vector<double> rp(m, 0.0);
+        for (int j = 0; j < N; ++j) {
+            if (x[j] == 0.0) continue;
+            if (j < n) { for (int e = h_cptr[j]; e < h_cptr[j + 1]; ++e) rp[h_crow[e]] += h_cval[e] * x[j]; }
+            else rp[j - n] += x[j];
+        }
+        double e4 = 0; for (double v : rp) e4 = std::max(e4, std::fabs(v));
+        fprintf(stderr, "[ds-x] %s it %d |Ax+s| %.3e\n", where, hc->iteration, e4);
+    }
+
+    // Profiling: one iteration at a time, every kernel bracketed by CUDA events.
+    int run_until_event_profiled() {
+        if (!pev[0]) for (auto& e : pev) CK(cudaEventCreate(&e));
+        while (true) {
+            pull();
+            if (opt.verbose >= 3) {
+                dbg_basis.resize(m);
+                CK(cudaMemcpyAsync(dbg_basis.data(), d_basis.p, sizeof(int) * m, cudaMemcpyDeviceToHost, stream));
+                CK(cudaStreamSynchronize(stream));
+            }
+            const int T0 = hc->T;
+            bool ran[S_NSTEPS] = {};
+            for (int stp = 0; stp < S_NSTEPS; ++stp) {
+                if ((stp == S_BTRAN_RHS || stp == S_FTRAN_K) && k == 0) continue;
+                CK(cudaEventRecord(pev[2 * stp], stream));
+                CK(launch_step(D, stp, stream));
+                CK(cudaEventRecord(pev[2 * stp + 1], stream));
+                ran[stp] = true;
+            }
+            pull();
+            if (hc->halt) return hc->event;
+            if (opt.verbose >= 3) { debug_check_iteration(); debug_check_representation("graph"); pull(); }
+            const bool dchk = (hc->iteration % NEED_RESTART) == 0;
+            for (int stp = 0; stp < S_NSTEPS; ++stp) {
+                if (!ran[stp]) continue;
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, pev[2 * stp], pev[2 * stp + 1]));
+                prof_us[stp] += 1000.0 * ms;
+                prof_bytes[stp] += step_bytes(stp, T0, hc->nrhs, dchk);
+                prof_n[stp] += 1;
+            }
+        }
+    }
+
     int run_until_event() {
+        if (prof || opt.verbose >= 3) return run_until_event_profiled();
         while (true) {
             ensure_graph();
             const int it = hc->iteration;
@@ -520,7 +704,7 @@ struct Engine {
             if (batch > BATCH_ITERS) batch = BATCH_ITERS;
             if (batch < 1) batch = 1;
             for (int b = 0; b < batch; ++b) CK(cudaGraphLaunch(gexec, stream));
-            st.kernel_launches += batch * 13;
+            count_launch((int)(batch * graph_nodes));
             pull();
             if (hc->halt) return hc->event;
         }
@@ -533,14 +717,34 @@ struct Engine {
             refactor(); phase1(); dual_simplex_init(); st.restarts++;
         }
         pull();
-        if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); }
+        if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); perturb_guard(); }
+    }
+
+    // Perturbing the basic costs moves y = B^-T c_B and can leave nonbasic reduced
+    // costs of the wrong sign; the reference then takes a step of the wrong sign
+    // until its next NEED_RESTART check.  Restore dual feasibility at once.
+    void perturb_guard() {
+        if (opt.strict_reference || dual_feasible()) return;
+        refactor(); phase1(); dual_simplex_init(); st.restarts++;
     }
 
     // Run the rest of the current iteration from pricing on (after a top event).
     int run_body_once() {
         pull(); clear_event(); push();
+        if (opt.verbose >= 3) {
+            debug_check_representation("before-body");
+            dbg_basis.resize(m);
+            CK(cudaMemcpyAsync(dbg_basis.data(), d_basis.p, sizeof(int) * m, cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            debug_check_x("before-body");
+        }
         CK(launch_body(D, ST_PRICING, stream));
         pull();
+        if (opt.verbose >= 3 && !hc->halt) {
+            fprintf(stderr, "[ds-body] it %d p %d p_idx %d q %d q_idx %d theta %.6e delta %.6e nrhs %d T %d\n", hc->iteration,
+                    hc->p, hc->p_idx, hc->q, hc->q_idx, hc->theta, hc->delta_bfrt, hc->nrhs, hc->T);
+            debug_check_iteration(); debug_check_representation("after-body"); pull();
+        }
         return hc->halt ? hc->event : EV_NONE;
     }
 
@@ -554,6 +758,10 @@ struct Engine {
         int pivots_at_nop = -1;
         int ev = run_until_event();
         while (true) {
+            if (opt.verbose) {
+                fprintf(stderr, "[ds] it %d event %d stage %d k %d T %d obj %.12g cycle %d pert %d\n", hc->iteration, ev,
+                        hc->event_stage, k, hc->T, hc->obj, hc->cycle, (int)perturbed);
+            }
             switch (ev) {
                 case EV_NONE: ev = run_until_event(); continue;
                 case EV_ITER_LIMIT: status = DS_STATUS_ITER_LIMIT; return false;
@@ -566,12 +774,13 @@ struct Engine {
                     clear_event(); push();
                     refactor(); phase1(); dual_simplex_init(); st.restarts++;
                     pull();
-                    if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); }
+                    if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); perturb_guard(); }
                     ev = run_body_once();
                     continue;
                 case EV_PERTURB:
                     clear_event(); push();
                     perturb(); refactor(); dual_simplex_init();
+                    perturb_guard();
                     ev = run_body_once();
                     continue;
                 case EV_OPTIMAL: status = DS_STATUS_OPTIMAL; return true;
@@ -611,6 +820,40 @@ struct Engine {
         }
     }
 
+    // Factorise the given basis and apply B^-1 (rows -> positions) or B^-T
+    // (positions -> rows) to nr dense vectors.
+    void basis_solve(const int* basis, const double* rhs, double* out, int nr, int transpose) {
+        if (!loaded) throw CudaError("basis_solve before load", DS_ERR_STATE);
+        std::vector<int> b(basis, basis + m), nb, vp(N, 0), seen(N, 0);
+        for (int v : b) { if (v < 0 || v >= N || seen[v]++) throw CudaError("bad basis", DS_ERR_ARG); }
+        for (int j = 0; j < N; ++j) if (!seen[j]) nb.push_back(j);
+        if ((int)nb.size() != n) throw CudaError("bad basis", DS_ERR_ARG);
+        for (int i = 0; i < m; ++i) vp[b[i]] = i;
+        for (int s2 = 0; s2 < n; ++s2) vp[nb[s2]] = -(s2 + 1);
+        std::memset(hc, 0, sizeof(Ctl));
+        hc->max_iter = 1; hc->R = 1; hc->phase = 2; hc->prev_q = -1; hc->ybt_n = -1;
+        sync_dev(); push();
+        CK(cudaMemcpyAsync(d_basis.p, b.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_nonbasis.p, nb.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_var_pos.p, vp.data(), sizeof(int) * N, cudaMemcpyHostToDevice, stream));
+        refactor();
+        DBuf<double> in, o;
+        in.alloc((size_t)nr * m); o.alloc((size_t)nr * m);
+        CK(cudaMemcpyAsync(in.p, rhs, sizeof(double) * nr * m, cudaMemcpyHostToDevice, stream));
+        for (int r0 = 0; r0 < nr; r0 += (transpose ? 1 : MAX_FTRAN_RHS)) {
+            if (transpose) {
+                btran_dense(in.p + (size_t)r0 * m, o.p + (size_t)r0 * m);
+            } else {
+                Dev E = D;
+                const int cnt = std::min(MAX_FTRAN_RHS, nr - r0);
+                for (int q = 0; q < cnt; ++q) { E.frhs[q] = in.p + (size_t)(r0 + q) * m; E.fout[q] = o.p + (size_t)(r0 + q) * m; }
+                CK(launch_ftran(E, cnt, 0, 1, stream));
+            }
+        }
+        CK(cudaMemcpyAsync(out, o.p, sizeof(double) * nr * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
     // presolve + solve + postProcess (tpp:5-30, 123-180) with the cleanup guard
     void solve() {
         if (!loaded) throw CudaError("solve before load", DS_ERR_STATE);
@@ -630,12 +873,14 @@ struct Engine {
         CK(cudaMemsetAsync(d_x.p, 0, sizeof(double) * N, stream));
         CK(cudaMemsetAsync(d_d.p, 0, sizeof(double) * N, stream));
         CK(cudaMemsetAsync(d_blocked.p, 0, N, stream));
+        CK(cudaMemsetAsync(d_aq.p, 0, sizeof(double) * m, stream));
         d_trace.alloc(2 * std::max(trace_cap, 1)); d_trace_d.alloc(2 * std::max(trace_cap, 1));
         std::memset(hc, 0, sizeof(Ctl));
         hc->max_iter = opt.max_iterations; hc->R = std::min(std::max(opt.refactor_interval, 1), cap - 5);
         hc->phase = 2; hc->prev_q = -1; hc->ybt_n = -1; hc->trace_cap = trace_cap;
         sync_dev();
         push();
+        const long long launches0 = launch_count();
         CK(cudaEventRecord(ev0, stream));
         try {
             refactor();                      // initDualSimplex (cudaDualSimplex.cpp:20-81)
@@ -672,6 +917,7 @@ struct Engine {
         CK(cudaStreamSynchronize(stream));
         float ms = 0; cudaEventElapsedTime(&ms, ev0, ev1);
         st.solve_ms = ms;
+        st.kernel_launches = (int)(launch_count() - launches0);
         pull();
         st.iterations = hc->iteration;
         st.learned_used = hc->learned_used;
@@ -849,6 +1095,45 @@ int ds_get_basis(const ds_solver* s, int* basis) {
 }
 
 const char* ds_last_error(const ds_solver* s) { return s ? s->last_error.c_str() : "null handle"; }
+
+long long ds_kernel_launch_count(void) { return ds::launch_count(); }
+
+int ds_basis_solve(ds_solver* s, const int* basis, const double* rhs, double* out, int nrhs, int transpose) {
+    if (!s || !basis || !rhs || !out || nrhs <= 0) return DS_ERR_ARG;
+    GUARD(s, { s->e->basis_solve(basis, rhs, out, nrhs, transpose); return DS_OK; })
+}
+
+int ds_profile_solve(ds_solver* s, char* json, int len) {
+    if (!s || !json || len <= 0) return DS_ERR_ARG;
+    Engine* e = s->e;
+    GUARD(s, {
+        for (int i = 0; i < ds::S_NSTEPS; ++i) { e->prof_us[i] = 0; e->prof_bytes[i] = 0; e->prof_n[i] = 0; }
+        e->prof = true;
+        try { e->solve(); } catch (...) { e->prof = false; throw; }
+        e->prof = false;
+        double tot = 0;
+        for (int i = 0; i < ds::S_NSTEPS; ++i) tot += e->prof_us[i];
+        std::string out = "{\"iterations\": " + std::to_string(e->st.iterations) + ", \"kernels\": [";
+        bool first = true;
+        for (int i = 0; i < ds::S_NSTEPS; ++i) {
+            if (e->prof_n[i] == 0) continue;
+            char buf[512];
+            const double avg_us = e->prof_us[i] / e->prof_n[i];
+            const double avg_b = e->prof_bytes[i] / e->prof_n[i];
+            snprintf(buf, sizeof(buf),
+                     "%s{\"name\": \"%s\", \"launches\": %lld, \"total_us\": %.3f, \"avg_us\": %.4f, "
+                     "\"bytes\": %.1f, \"gbs\": %.2f, \"share\": %.5f}",
+                     first ? "" : ", ", ds::kStepNames[i], e->prof_n[i], e->prof_us[i], avg_us, avg_b,
+                     avg_b / (avg_us * 1e-6) / 1e9, tot > 0 ? e->prof_us[i] / tot : 0.0);
+            out += buf;
+            first = false;
+        }
+        out += "]}";
+        if ((int)out.size() + 1 > len) return fail(s, DS_ERR_CAPACITY, "profile buffer too small");
+        std::memcpy(json, out.c_str(), out.size() + 1);
+        return DS_OK;
+    })
+}
 
 int ds_set_trace(ds_solver* s, int cap) {
     if (!s || cap < 0) return DS_ERR_ARG;

@@ -9,8 +9,9 @@
 //                    an explicit inverse Kinv (column major); slack columns of
 //                    the basis are unit vectors and are eliminated exactly.
 //   Eta file:        up to cap dense columns of m doubles + pivot positions, and
-//                    Mtri = (I - G)^-1 (cap x cap) which turns the sequential
-//                    product-form chain into one streaming pass.
+//                    G (cap x cap, G[t][u] = eta_u[p_t] - [p_u == p_t]): the
+//                    chain's pivot values come from a small triangular solve,
+//                    after which the eta columns are applied in one streaming pass.
 //   Control:         a small Ctl block; every kernel of an iteration reads the
 //                    decisions of the previous kernels from it and returns at
 //                    once when a previous kernel raised an event.
@@ -99,7 +100,7 @@ struct Dev {
     int* cpl_ptr; int* cpl_col; double* cpl_val;                // coupling A[R, S] by rows
     double* Kinv;                                               // k*k column major
     // eta file
-    double* eta; int* eta_pos; double* Mtri;
+    double* eta; int* eta_pos; double* Mtri;                    // Mtri holds G (row t: G[t][0..t-1])
     // work vectors
     double* rho;        // m (rows)
     double* alpha;      // n (nonbasic slots), un-negated pivot row

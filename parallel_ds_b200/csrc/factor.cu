@@ -76,7 +76,7 @@ __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double*
             double bv = -1.0; int b = -1;
             for (int u = 0; u < BS / 32; ++u)
                 if (red_v[u] > bv || (red_v[u] == bv && red_i[u] >= 0 && (b < 0 || red_i[u] < b))) { bv = red_v[u]; b = red_i[u]; }
-            if (b < 0 || !(bv > 1e-300)) { *err = 1; b = -1; }
+            if (b < 0 || !(bv > 1e-300)) { *err = c0 + a + 1; b = -1; }
             else { rowpiv[b] = c0 + a; piv_rows[c0 + a] = b; }
             s_r = b;
         }
@@ -202,6 +202,7 @@ cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s
     }
     dim3 g((k + 31) / 32, (k + 31) / 32), b(32, 32);
     k_gj_permute<<<g, b, 0, s>>>(F.S, k, F.piv_rows, D.Kinv);
+    count_launch(3 + 3 * ((k + GJ_NB - 1) / GJ_NB));
     return cudaGetLastError();
 }
 

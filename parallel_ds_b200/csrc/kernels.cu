@@ -26,6 +26,7 @@
 //
 // Arithmetic that decides indices follows the reference's operation order
 // exactly and the file is compiled with -fmad=false.
+#include <atomic>
 #include <cfloat>
 #include <climits>
 #include <cmath>
@@ -233,8 +234,36 @@ __global__ void k_dual_check(Dev D, int force) {
     if (last_block(&c->tickets[1]) && threadIdx.x == 0) {
         if (force) return;
         c->need_dual_check = 0;
-        if (c->dual_infeas > 0) raise_ev(c, EV_DUALINF, ST_TOP);
+        if (atomicAdd(&c->dual_infeas, 0) > 0) raise_ev(c, EV_DUALINF, ST_TOP);
         else if (!c->perturbed && c->cycle > MAX_CYCLE) raise_ev(c, EV_PERTURB, ST_TOP);
+    }
+}
+
+// ================================================================ eta chain
+// G[t][u] = eta_u[p_t] - [p_u == p_t] (u < t) couples the product-form factors.
+// FTRAN needs s_t = g_t + sum_{u<t} G[t][u] s_u (s_t is the pivot entry the
+// sequential product form reads before applying eta t); BTRAN needs
+// d_t = h_t + sum_{u>t} G[u][t] d_u.  One warp walks the chain; each step's dot
+// product is spread over the lanes and reduced by shuffles (fixed order).
+__device__ void eta_forward(const Dev& D, const double* g, double* s, int T) {
+    const int lane = threadIdx.x & 31;
+    for (int t = 0; t < T; ++t) {
+        const double* Gr = D.Mtri + (size_t)t * D.cap;
+        double v = 0.0;
+        for (int u = lane; u < t; u += 32) v += Gr[u] * s[u];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) s[t] = g[t] + v;
+        __syncwarp();
+    }
+}
+__device__ void eta_backward(const Dev& D, const double* h, double* dl, int T) {
+    const int lane = threadIdx.x & 31;
+    for (int t = T - 1; t >= 0; --t) {
+        double v = 0.0;
+        for (int u = t + 1 + lane; u < T; u += 32) v += D.Mtri[(size_t)u * D.cap + t] * dl[u];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) dl[t] = h[t] + v;
+        __syncwarp();
     }
 }
 
@@ -258,11 +287,7 @@ __device__ void btran_unit_eta(const Dev& D, int p_idx) {
     for (int t = threadIdx.x; t < T; t += BS)
         h[t] = D.eta[(size_t)t * D.m + p_idx] - (D.eta_pos[t] == p_idx ? 1.0 : 0.0);
     __syncthreads();
-    for (int t = threadIdx.x; t < T; t += BS) {
-        double s = 0.0;
-        for (int v = t; v < T; ++v) s += D.Mtri[(size_t)v * D.cap + t] * h[v];
-        dl[t] = s;
-    }
+    if (threadIdx.x < 32) eta_backward(D, h, dl, T);
     __syncthreads();
     if (threadIdx.x == 0) {
         D.ybt[p_idx] = 1.0;
@@ -319,8 +344,8 @@ __global__ void k_chuzr(Dev D) {
     ArgMax v{-1.0, INT_MAX};
     int tot = 0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
-        v = better_max(v, ArgMax{D.red[b], D.redi[b]});
-        tot += D.redi[gridDim.x + b];
+        v = better_max(v, ArgMax{__ldcg(&D.red[b]), __ldcg(&D.redi[b])});
+        tot += __ldcg(&D.redi[gridDim.x + b]);
     }
     v = block_argmax<BS>(v);
     tot = block_sum_int<BS>(tot);
@@ -414,13 +439,13 @@ __device__ void rt_full_scan(const Dev& D, double sgn_a, int* q_idx_out) {
     double theta = INF_THETA;
     int q_idx = -1;
     for (int i = 0; i < D.n; ++i) {
-        if (!D.cand[i]) continue;
-        const double th = D.theta_arr[i];
+        if (!__ldcg(&D.cand[i])) continue;
+        const double th = __ldcg(&D.theta_arr[i]);
         if (isnan(th)) continue;   // removed by BFRT or not takeable
-        const double a = sgn_a * D.alpha[i];
+        const double a = sgn_a * __ldcg(&D.alpha[i]);
         if (th < theta) { theta = th; q_idx = i; }
         else if (q_idx >= 0 && fabs(th - theta) < EPS_Z) {
-            if (fabs(a) > fabs(sgn_a * D.alpha[q_idx])) { theta = th; q_idx = i; }
+            if (fabs(a) > fabs(sgn_a * __ldcg(&D.alpha[q_idx]))) { theta = th; q_idx = i; }
         }
     }
     *q_idx_out = q_idx;
@@ -442,8 +467,8 @@ __device__ int rt_select(const Dev& D, double sgn_a) {
     // global first minimiser over takeable candidates
     ArgMin v{CUDART_INF, INT_MAX};
     for (int i = threadIdx.x; i < D.n; i += BS) {
-        const double th = D.theta_arr[i];
-        if (D.cand[i] && !isnan(th)) v = better_min(v, ArgMin{th, i});
+        const double th = __ldcg(&D.theta_arr[i]);
+        if (__ldcg(&D.cand[i]) && !isnan(th)) v = better_min(v, ArgMin{th, i});
     }
     (void)s_tmin; (void)s_imin;
     v = block_argmin<BS>(v);
@@ -460,8 +485,8 @@ __device__ int rt_select(const Dev& D, double sgn_a) {
     for (int base = istar + 1; base < D.n; base += BS) {
         const int i = base + threadIdx.x;
         bool mem = false;
-        if (i < D.n && D.cand[i]) {
-            const double th = D.theta_arr[i];
+        if (i < D.n && __ldcg(&D.cand[i])) {
+            const double th = __ldcg(&D.theta_arr[i]);
             mem = !isnan(th) && th <= B;
         }
         const unsigned ball = __ballot_sync(0xffffffffu, mem);
@@ -485,17 +510,17 @@ __device__ int rt_select(const Dev& D, double sgn_a) {
     }
     if (threadIdx.x == 0) {
         int q = istar;
-        double theta = D.theta_arr[istar];
+        double theta = __ldcg(&D.theta_arr[istar]);
         double maxrun = theta;
         bool exact = !overflow;
         if (exact) {
             for (int u = 0; u < nlist; ++u) {
                 const int i = list[u];
-                const double th = D.theta_arr[i];
-                const double a = sgn_a * D.alpha[i];
+                const double th = __ldcg(&D.theta_arr[i]);
+                const double a = sgn_a * __ldcg(&D.alpha[i]);
                 if (th < theta) { theta = th; q = i; }
                 else if (fabs(th - theta) < EPS_Z) {
-                    if (fabs(a) > fabs(sgn_a * D.alpha[q])) { theta = th; q = i; }
+                    if (fabs(a) > fabs(sgn_a * __ldcg(&D.alpha[q]))) { theta = th; q = i; }
                 }
                 if (theta > maxrun) maxrun = theta;
             }
@@ -557,7 +582,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
     if (!last_block(&c->tickets[3])) return;
     __shared__ int s_tot, s_q;
     int tot = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += D.redi[b];
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += __ldcg(&D.redi[b]);
     tot = block_sum_int<BS>(tot);
     if (threadIdx.x == 0) {
         s_tot = tot;
@@ -580,11 +605,11 @@ __global__ void k_pivot_row(Dev D, int mode) {
         if (phase != 2) break;
         const int qv = D.nonbasis[q_idx];
         if (D.type[qv] != BOXED) break;
-        const double span = (D.ub[qv] - D.lb[qv]) * fabs(sgn_a * D.alpha[q_idx]);
+        const double span = (D.ub[qv] - D.lb[qv]) * fabs(sgn_a * __ldcg(&D.alpha[q_idx]));
         if (delta - span <= 0) break;
         delta -= span;
         __syncthreads();
-        if (threadIdx.x == 0) D.theta_arr[q_idx] = CUDART_NAN;   // F.erase(q_idx)
+        if (threadIdx.x == 0) __stcg(&D.theta_arr[q_idx], CUDART_NAN);   // F.erase(q_idx)
         --remaining;
         __syncthreads();
         if (remaining == 0) break;
@@ -593,7 +618,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
         if (q_idx < 0) { c->err = 1; raise_ev(c, EV_ERROR, ST_RATIO); return; }
         const int qv = D.nonbasis[q_idx];
         c->q = qv; c->q_idx = q_idx;
-        c->theta = D.d[qv] / D.alpha[q_idx];
+        c->theta = D.d[qv] / __ldcg(&D.alpha[q_idx]);
         c->delta_bfrt = (c->is_lower ? -1.0 : 1.0) * delta;
         if (phase == 1) {
             // infisibilityCorr(q) (tpp:614-625) on d before the update
@@ -637,7 +662,7 @@ __global__ void k_dual_update(Dev D) {
     if (!last_block(&c->tickets[4])) return;
     __shared__ int s_nf;
     int tot = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += D.redi[b];
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += __ldcg(&D.redi[b]);
     tot = block_sum_int<BS>(tot);
     if (threadIdx.x == 0) {
         s_nf = tot;
@@ -667,7 +692,7 @@ __global__ void k_dual_update(Dev D) {
         double dz = 0.0;
         int nl = 0;
         for (int s = 0; s < D.n; ++s) {
-            const unsigned char fl = D.flip[s];
+            const unsigned char fl = __ldcg(&D.flip[s]);
             if (!fl) continue;
             const int j = D.nonbasis[s];
             const double span = D.ub[j] - D.lb[j];
@@ -762,7 +787,7 @@ __global__ void k_ftran_k2(Dev D, int nr_fixed, int force) {
         const int pos = D.s_pos[j];
         for (int r = 0; r < nr; ++r) {
             double s = 0.0;
-            for (int ch = 0; ch < (int)gridDim.y; ++ch) s += D.ftr_part[(size_t)ch * MAX_FTRAN_RHS * k + r * k + j];
+            for (int ch = 0; ch < (int)gridDim.y; ++ch) s += __ldcg(&D.ftr_part[(size_t)ch * MAX_FTRAN_RHS * k + r * k + j]);
             D.y0[r][pos] = s;
         }
     }
@@ -789,18 +814,16 @@ __global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
     }
     if (!last_block(&c->tickets[5])) return;
     const int T = c->T;
-    __shared__ double g[MAX_FTRAN_RHS][1024];
+    __shared__ double g[MAX_FTRAN_RHS][256];
+    __shared__ double sv[MAX_FTRAN_RHS][256];
     for (int t = threadIdx.x; t < T; t += BS)
-        for (int q = 0; q < nr; ++q) g[q][t] = D.y0[q][D.eta_pos[t]];
+        for (int q = 0; q < nr; ++q) g[q][t] = __ldcg(&D.y0[q][D.eta_pos[t]]);
     __syncthreads();
-    for (int t = threadIdx.x; t < T; t += BS) {
-        const double* Mrow = D.Mtri + (size_t)t * D.cap;
-        for (int q = 0; q < nr; ++q) {
-            double s = 0.0;
-            for (int v = 0; v <= t; ++v) s += Mrow[v] * g[q][v];
-            D.s_eta[q * D.cap + t] = s;
-        }
-    }
+    const int w = threadIdx.x >> 5;
+    if (w < nr) eta_forward(D, g[w], sv[w], T);
+    __syncthreads();
+    for (int t = threadIdx.x; t < T; t += BS)
+        for (int q = 0; q < nr; ++q) D.s_eta[q * D.cap + t] = sv[q][t];
 }
 
 // y = y0 + sum_t s_t eta_t (streaming over the eta file); the last block applies
@@ -837,10 +860,10 @@ __global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
         for (int q = 0; q < nr; ++q)
             for (int t = 0; t < T; ++t) {
                 const int pt = D.eta_pos[t];
-                D.fout[q][pt] = D.fout[q][pt] - s[q][t];
+                D.fout[q][pt] = __ldcg(&D.fout[q][pt]) - s[q][t];
             }
         if (check) {
-            const double aqp = D.fout[0][c->p_idx];
+            const double aqp = __ldcg(&D.fout[0][c->p_idx]);
             const double apq = D.alpha[c->q_idx];
             if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
             else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
@@ -891,7 +914,7 @@ __global__ void k_update(Dev D, int force) {
         D.beta[p_idx] = bp / (ap * ap);
         if (phase == 2) {
             double dz = c->dz;
-            if (nflips > 0) for (int b = 0; b < (int)gridDim.x; ++b) dz -= D.red[b];
+            if (nflips > 0) for (int b = 0; b < (int)gridDim.x; ++b) dz -= __ldcg(&D.red[b]);
             c->obj += dz;
             D.x[q] = D.x[q] + theta_P;
         } else {
@@ -925,15 +948,11 @@ __global__ void k_update(Dev D, int force) {
         }
         if (phase == 2) c->trace_n += 1;
     }
-    // new row of Mtri: G[T][u] = eta_u[p_T] - [p_u == p_T],  M[T][v] = [v == T] + sum_u G[T][u] M[u][v]
+    // new row of G: G[T][u] = eta_u[p_T] - [p_u == p_T]
     for (int u = threadIdx.x; u < T; u += BS)
         g[u] = D.eta[(size_t)u * D.m + p_idx] - (D.eta_pos[u] == p_idx ? 1.0 : 0.0);
     __syncthreads();
-    for (int v = threadIdx.x; v <= T; v += BS) {
-        double s = (v == T) ? 1.0 : 0.0;
-        for (int u = v; u < T; ++u) s += g[u] * D.Mtri[(size_t)u * D.cap + v];
-        D.Mtri[(size_t)T * D.cap + v] = s;
-    }
+    for (int u = threadIdx.x; u < T; u += BS) D.Mtri[(size_t)T * D.cap + u] = g[u];
     __syncthreads();
     if (threadIdx.x == 0) {
         c->T = T + 1;
@@ -1018,11 +1037,10 @@ __global__ void k_btran_dense_fix(Dev D, const double* c0, const double* h) {
     __shared__ double dl[1024];
     const int T = D.ctl->T;
     for (int i = threadIdx.x; i < D.m; i += BS) D.ybt[i] = c0[i];
-    for (int t = threadIdx.x; t < T; t += BS) {
-        double s = 0.0;
-        for (int v = t; v < T; ++v) s += D.Mtri[(size_t)v * D.cap + t] * h[v];
-        dl[t] = s;
-    }
+    __shared__ double hs[1024];
+    for (int t = threadIdx.x; t < T; t += BS) hs[t] = h[t];
+    __syncthreads();
+    if (threadIdx.x < 32) eta_backward(D, hs, dl, T);
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int t = 0; t < T; ++t) { const int pt = D.eta_pos[t]; D.ybt[pt] = D.ybt[pt] + dl[t]; }
@@ -1089,12 +1107,12 @@ __global__ void k_count_dual_inf(Dev D) {
     if (threadIdx.x == 0) D.redi[blockIdx.x] = bad;
     if (!last_block(&c->tickets[8])) return;
     int tot = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += D.redi[b];
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += __ldcg(&D.redi[b]);
     tot = block_sum_int<BS>(tot);
     if (threadIdx.x == 0) c->p1_dinf = tot;
 }
 
-// Mtri for an eta file given column by column (one block, rows in order).
+// G for an eta file given column by column (one block, rows in order).
 template <int BS>
 __global__ void k_build_mtri(Dev D, int T) {
     __shared__ double g[1024];
@@ -1103,11 +1121,7 @@ __global__ void k_build_mtri(Dev D, int T) {
         for (int u = threadIdx.x; u < t; u += BS)
             g[u] = D.eta[(size_t)u * D.m + pt] - (D.eta_pos[u] == pt ? 1.0 : 0.0);
         __syncthreads();
-        for (int v = threadIdx.x; v <= t; v += BS) {
-            double s = (v == t) ? 1.0 : 0.0;
-            for (int u = v; u < t; ++u) s += g[u] * D.Mtri[(size_t)u * D.cap + v];
-            D.Mtri[(size_t)t * D.cap + v] = s;
-        }
+        for (int u = threadIdx.x; u < t; u += BS) D.Mtri[(size_t)t * D.cap + u] = g[u];
         __syncthreads();
     }
     if (threadIdx.x == 0) D.ctl->T = T;
@@ -1115,6 +1129,12 @@ __global__ void k_build_mtri(Dev D, int T) {
 
 // ================================================================= launchers
 constexpr int BS = 256;
+
+static std::atomic<long long> g_launches{0};
+static thread_local bool g_counting_off = false;
+void count_launch(int nk) { if (!g_counting_off) g_launches.fetch_add(nk, std::memory_order_relaxed); }
+void set_launch_counting(bool on) { g_counting_off = !on; }
+long long launch_count() { return g_launches.load(); }
 static inline int nblk(int n) { return (n + BS - 1) / BS; }
 
 #define LAUNCH_OK() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
@@ -1122,18 +1142,21 @@ static inline int nblk(int n) { return (n + BS - 1) / BS; }
 cudaError_t launch_top(const Dev& D, cudaStream_t s) {
     k_top<<<1, 32, 0, s>>>(D);
     k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 0);
+    count_launch(2);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_dual_check(const Dev& D, cudaStream_t s) {
     k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 1);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_count_dual_inf(const Dev& D, cudaStream_t s) {
     k_count_dual_inf<BS><<<nblk(D.n), BS, 0, s>>>(D);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
@@ -1142,6 +1165,7 @@ cudaError_t launch_btran_b0(const Dev& D, double* out, int force, cudaStream_t s
     if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, force);
     const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
     k_btran_gemv<BS><<<nbw + nblk(D.m), BS, 0, s>>>(D, out, force);
+    count_launch((D.k > 0 ? 1 : 0) + 1);
     LAUNCH_OK();
     return cudaSuccess;
 }
@@ -1154,63 +1178,102 @@ cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaS
     }
     k_ftran_assemble<BS><<<nblk(D.m), BS, 0, s>>>(D, nr_fixed, force);
     k_eta_apply<BS><<<nblk(D.m), BS, 0, s>>>(D, nr_fixed, check, force);
+    count_launch((D.k > 0 ? 1 : 0) + 2);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
+// One kernel of the iteration sequence (profiling launches them one by one).
+const char* const kStepNames[S_NSTEPS] = {"k_top", "k_dual_check", "k_chuzr", "k_btran_rhs", "k_btran_gemv",
+                                          "k_pivot_row", "k_dual_update", "k_ftran_k", "k_ftran_assemble",
+                                          "k_eta_apply", "k_update"};
+
+cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
+    switch (step) {
+        case S_TOP: k_top<<<1, 32, 0, s>>>(D); break;
+        case S_DUALCHECK: k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 0); break;
+        case S_CHUZR: k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D); break;
+        case S_BTRAN_RHS: if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, 0); else return cudaSuccess; break;
+        case S_BTRAN_GEMV: {
+            const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
+            k_btran_gemv<BS><<<nbw + nblk(D.m), BS, 0, s>>>(D, D.rho, 0);
+            break;
+        }
+        case S_PIVOT_ROW: k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, 3); break;
+        case S_DUAL_UPDATE: k_dual_update<BS><<<nblk(D.n), BS, 0, s>>>(D); break;
+        case S_FTRAN_K:
+            if (D.k > 0) {
+                dim3 g(D.ftr_ntile, D.ftr_nchunk);
+                const size_t sh = (size_t)D.ftr_chunk * MAX_FTRAN_RHS * sizeof(double);
+                k_ftran_k2<BS><<<g, BS, sh, s>>>(D, 0, 0);
+            } else {
+                return cudaSuccess;
+            }
+            break;
+        case S_FTRAN_ASM: k_ftran_assemble<BS><<<nblk(D.m), BS, 0, s>>>(D, 0, 0); break;
+        case S_ETA_APPLY: k_eta_apply<BS><<<nblk(D.m), BS, 0, s>>>(D, 0, 1, 0); break;
+        case S_UPDATE: k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 0); break;
+        default: return cudaErrorInvalidValue;
+    }
+    count_launch(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_body(const Dev& D, int from_stage, cudaStream_t s) {
-    if (from_stage <= ST_PRICING) {
-        k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D);
-        cudaError_t e = launch_btran_b0(D, D.rho, 0, s);
-        if (e != cudaSuccess) return e;
-        k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, 3);
-        k_dual_update<BS><<<nblk(D.n), BS, 0, s>>>(D);
-        e = launch_ftran(D, 0, 1, 0, s);
+    const int first = (from_stage <= ST_PRICING) ? S_CHUZR : S_UPDATE;
+    for (int st = first; st < S_NSTEPS; ++st) {
+        cudaError_t e = launch_step(D, st, s);
         if (e != cudaSuccess) return e;
     }
-    k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 0);
-    LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_update_forced(const Dev& D, cudaStream_t s) {
     k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 1);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_iteration(const Dev& D, cudaStream_t s) {
-    cudaError_t e = launch_top(D, s);
-    if (e != cudaSuccess) return e;
-    return launch_body(D, ST_PRICING, s);
+    for (int st = S_TOP; st < S_NSTEPS; ++st) {
+        cudaError_t e = launch_step(D, st, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t launch_set_primal_vars(const Dev& D, cudaStream_t s) {
     k_set_primal_vars<<<nblk(D.n), BS, 0, s>>>(D);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_xb_rhs(const Dev& D, double* rhs, cudaStream_t s) {
     k_xb_rhs<<<nblk(D.m), BS, 0, s>>>(D, rhs);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_scatter_basic(const Dev& D, const double* xb, double* dst, cudaStream_t s) {
     k_scatter_basic<<<nblk(D.m), BS, 0, s>>>(D, xb, dst);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_gather_basic_cost(const Dev& D, double* cb, cudaStream_t s) {
     k_gather_basic_cost<<<nblk(D.m), BS, 0, s>>>(D, cb);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_reduced_costs(const Dev& D, const double* y, cudaStream_t s) {
     k_reduced_costs<<<nblk(D.n), BS, 0, s>>>(D, y);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
@@ -1218,48 +1281,56 @@ cudaError_t launch_reduced_costs(const Dev& D, const double* y, cudaStream_t s) 
 cudaError_t launch_btran_dense_eta(const Dev& D, const double* c0, double* h, int T, cudaStream_t s) {
     if (T > 0) k_eta_dots<BS><<<T, BS, 0, s>>>(D, c0, h);
     k_btran_dense_fix<BS><<<1, BS, 0, s>>>(D, c0, h);
+    count_launch((T > 0 ? 1 : 0) + 1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_btran_unit(const Dev& D, int p_idx, cudaStream_t s) {
     k_btran_unit<BS><<<1, BS, 0, s>>>(D, p_idx);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_norm2(const double* v, int n, double* out, cudaStream_t s) {
     k_norm2<BS><<<1, BS, 0, s>>>(v, n, out);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_dot_cost_x(const Dev& D, double* out, cudaStream_t s) {
     k_dot_cost_x<BS><<<1, BS, 0, s>>>(D, out);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_build_mtri(const Dev& D, int T, cudaStream_t s) {
     k_build_mtri<BS><<<1, BS, 0, s>>>(D, T);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_chuzr_only(const Dev& D, cudaStream_t s) {
     k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_pivot_row_mode(const Dev& D, int mode, cudaStream_t s) {
     k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, mode);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_phase1_init(const Dev& D, double* cc, cudaStream_t s) {
     k_phase1_init<BS><<<1, BS, 0, s>>>(D, cc);
+    count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;
 }

@@ -20,6 +20,17 @@ struct FactorBufs {
 
 cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s);
 
+// Kernels of one iteration, in launch order.
+enum Step : int { S_TOP = 0, S_DUALCHECK, S_CHUZR, S_BTRAN_RHS, S_BTRAN_GEMV, S_PIVOT_ROW, S_DUAL_UPDATE,
+                  S_FTRAN_K, S_FTRAN_ASM, S_ETA_APPLY, S_UPDATE, S_NSTEPS };
+extern const char* const kStepNames[S_NSTEPS];
+cudaError_t launch_step(const Dev& D, int step, cudaStream_t s);
+
+// Kernel launch accounting (graph replays are added by the caller).
+void count_launch(int nk);
+void set_launch_counting(bool on);
+long long launch_count();
+
 cudaError_t launch_top(const Dev& D, cudaStream_t s);
 cudaError_t launch_body(const Dev& D, int from_stage, cudaStream_t s);
 cudaError_t launch_iteration(const Dev& D, cudaStream_t s);

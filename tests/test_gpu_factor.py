@@ -1,0 +1,100 @@
+"""GPU refactorisation + FTRAN/BTRAN against dense numpy solves.
+
+Bases come from the oracle's own trajectory (so they are the nonsingular bases
+the dual simplex visits), at several iteration counts so that the structural
+block k spans small to large sizes.  Tolerance: 1e-10 relative to the solution
+scale (the bases have condition numbers around 1e3-1e4)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+from parallel_ds_b200 import lp as L
+from parallel_ds_b200._lib import lib, ptr
+
+pytestmark = pytest.mark.gpu
+
+
+def dense_basis(lp, basis):
+    m, n = lp["m"], lp["n"]
+    A = L.to_scipy(lp).toarray()
+    B = np.zeros((m, m))
+    for i, v in enumerate(basis):
+        if v < n:
+            B[:, i] = A[:, v]
+        else:
+            B[v - n, i] = 1.0
+    return B
+
+
+def gpu_solve(lp, basis, rhs, transpose):
+    t = L.typed(lp)
+    L_ = lib()
+    h = C.c_void_p()
+    assert L_.ds_create(None, C.byref(h)) == 0
+    try:
+        rc = L_.ds_load_typed(h, t["m"], t["n"], ptr(t["row_ptr"], C.c_int), ptr(t["col_idx"], C.c_int),
+                              ptr(t["val"], C.c_double), ptr(t["c"], C.c_double), ptr(t["col_type"], C.c_int),
+                              ptr(t["col_lb"], C.c_double), ptr(t["col_ub"], C.c_double),
+                              ptr(t["row_type"], C.c_int), ptr(t["row_lb"], C.c_double),
+                              ptr(t["row_ub"], C.c_double))
+        assert rc == 0
+        b = np.ascontiguousarray(basis, np.int32)
+        r = np.ascontiguousarray(rhs.T if rhs.ndim == 2 else rhs[None, :], np.float64)
+        out = np.zeros_like(r)
+        rc = L_.ds_basis_solve(h, ptr(b, C.c_int), ptr(r, C.c_double), ptr(out, C.c_double), r.shape[0],
+                               int(transpose))
+        assert rc == 0, L_.ds_last_error(h)
+    finally:
+        L_.ds_destroy(h)
+    return out.T if rhs.ndim == 2 else out[0]
+
+
+@pytest.fixture(scope="module")
+def learned_bases():
+    lp = L.learned(0)
+    t = L.typed(lp)
+    out = []
+    for it in (1, 150, 300, 376, 700, 1500):
+        r = po.solve_typed(t, max_iterations=it)
+        out.append((it, r["basis"]))
+    return lp, out
+
+
+@pytest.mark.parametrize("transpose", [0, 1])
+def test_basis_solve_dense_rhs(learned_bases, transpose):
+    lp, bases = learned_bases
+    rng = np.random.default_rng(1)
+    for it, basis in bases:
+        B = dense_basis(lp, basis)
+        rhs = rng.standard_normal((lp["m"], 3))
+        ref = np.linalg.solve(B.T if transpose else B, rhs)
+        got = gpu_solve(lp, basis, rhs, transpose)
+        k = int((basis < lp["n"]).sum())
+        err = np.abs(got - ref).max() / max(1.0, np.abs(ref).max())
+        assert err <= 1e-10, (it, k, err)
+
+
+def test_basis_solve_sparse_and_unit_rhs(learned_bases):
+    lp, bases = learned_bases
+    A = L.to_scipy(lp).tocsc()
+    for it, basis in bases[1:]:
+        B = dense_basis(lp, basis)
+        cols = [A[:, j].toarray().ravel() for j in (0, 17, 3999)] + [np.eye(lp["m"])[5]]
+        rhs = np.stack(cols, axis=1)
+        ref = np.linalg.solve(B, rhs)
+        got = gpu_solve(lp, basis, rhs, 0)
+        err = np.abs(got - ref).max() / max(1.0, np.abs(ref).max())
+        assert err <= 1e-10, (it, err)
+
+
+@pytest.mark.parametrize("nr", [1, 2, 3, 4, 5])
+def test_basis_solve_rhs_counts(learned_bases, nr):
+    lp, bases = learned_bases
+    it, basis = bases[3]
+    B = dense_basis(lp, basis)
+    rhs = np.random.default_rng(nr).standard_normal((lp["m"], nr))
+    ref = np.linalg.solve(B, rhs)
+    got = gpu_solve(lp, basis, rhs, 0)
+    assert np.abs(got - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
