@@ -186,6 +186,26 @@ int ds_kernel_ratio_test(int n, int N, const int* nonbasis, const double* alpha,
                          int* q, int* q_idx, double* theta, double* delta_out,
                          int* num_candidates);
 
+/* Ratio test that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: a host framework that
+ * owns all device memory through its own pool, a latency-critical loop where
+ * cudaMalloc/cudaFree would stall the device, or a host callback, where CUDA
+ * allocation calls are not allowed.  Same kernel and results as
+ * ds_kernel_ratio_test, but every array argument is a DEVICE pointer the caller
+ * owns (type: one byte per variable, DS_* codes) and the outputs are host
+ * scalars.  Scratch lives in a fixed array of about 0.6 MB that every GPU
+ * loading this library holds until exit; n > DS_NOALLOC_MAX_SLOTS returns
+ * DS_ERR_CAPACITY.  The first call on a device looks up that array's device
+ * address, so make it before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other threads, other streams) race.  stream
+ * may be NULL; the call returns after its stream has synchronised. */
+#define DS_NOALLOC_MAX_SLOTS 65536
+int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, const double* alpha,
+                                 double delta, int is_lower, const double* x, const double* d,
+                                 const double* lb, const double* ub, const unsigned char* type,
+                                 int* q, int* q_idx, double* theta, double* delta_out,
+                                 int* num_candidates, void* stream);
+
 /* PFI eta file: linalg::PFIsolve (linalg.cpp:12-46) / etaSolveKernel
  * (cudaKernels.cu:266-322): apply T eta columns (eta[t*m + i], pivots pos[t])
  * forward (transpose=0) or backward (transpose=1) to rhs, result in sol. */
