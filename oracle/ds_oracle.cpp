@@ -568,7 +568,8 @@ struct Oracle {
             for (int i = 0; i < m; ++i) {
                 auto [inf, dt] = var_infeas(basis[i]);
                 if (inf && std::fabs(dt) > 1e-8) {
-                    const double w = (dt * dt) / beta[i];
+                    double w = (dt * dt) / beta[i];
+                    if (opt.var_weight) w *= opt.var_weight[basis[i]];
                     if (w > maxw) { p = basis[i]; p_idx = i; delta = dt; maxw = w; is_lower = dt < 0; }
                 }
             }
@@ -704,6 +705,7 @@ void or_default_options(or_options* o) {
     o->seed = 12345;
     o->gpu_control_flow = 1;
     o->verbose = 0;
+    o->var_weight = nullptr;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,

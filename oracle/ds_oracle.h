@@ -24,6 +24,8 @@ typedef struct or_options {
     unsigned long long seed;    /* perturbation seed                            */
     int gpu_control_flow;       /* 1: follow cudaDualSimplex.cpp's restarts     */
     int verbose;
+    const double* var_weight;   /* experiments: DSE score of row i is multiplied by
+                                   var_weight[basis[i]] (NULL: plain DSE)          */
 } or_options;
 
 typedef struct or_result {

@@ -194,14 +194,15 @@ struct Engine {
         d_s_pos.ensure(m); d_s_var.ensure(m); d_rp_row.ensure(m); d_pos_kidx.ensure(m);
         d_row_slackpos.ensure(m); d_row_kidx.ensure(m);
         d_cpl_ptr.ensure(m + 1); d_cpl_col.ensure(std::max(nnz, 1)); d_cpl_val.ensure(std::max(nnz, 1));
-        cap = std::min(std::max(opt.refactor_interval, 1), 240) + 5;
+        cap = std::min(std::max(opt.refactor_interval, 1), 200) + 5;
+        CK(init_kernel_attributes(cap));
         d_eta.ensure((size_t)cap * m); d_Mtri.ensure((size_t)cap * cap); d_eta_pos.ensure(cap); d_ybt_pos.ensure(cap + 1);
         d_rho.ensure(m); d_alpha.ensure(n); d_theta.ensure(n); d_cand.ensure(n); d_ybt.ensure(m);
         d_btr_rhs.ensure(m); d_aq.ensure(m); d_cc.ensure(m); d_alpha_q.ensure(m); d_tau.ensure(m); d_dxb.ensure(m);
         for (auto& b : d_y0) b.ensure(m);
         d_seta.ensure((size_t)MAX_FTRAN_RHS * cap);
         const int nb = std::max((m + 255) / 256, (n + 255) / 256) + 8;
-        d_red.ensure(2 * nb); d_redi.ensure(2 * nb);
+        d_red.ensure(2 * nb); d_redi.ensure(4 * nb);
         d_flip.ensure(n); d_flip_list.ensure(n);
         d_tmp_rows.ensure(m); d_tmp_rows2.ensure(m); d_tmp_pos.ensure(m); d_tmp_pos2.ensure(m); d_h.ensure(cap);
         d_ctl.ensure(1);
@@ -422,6 +423,12 @@ struct Engine {
             CK(cudaStreamSynchronize(stream));
             return;
         }
+        pull();
+        if (hc->T == 0) {            // every caller refactors first: B = B0
+            CK(launch_beta_exact(D, stream));
+            CK(cudaStreamSynchronize(stream));
+            return;
+        }
         for (int i = 0; i < m; ++i) {
             CK(launch_btran_unit(D, i, stream));
             CK(launch_btran_b0(D, d_tmp_rows.p, 1, stream));
@@ -563,9 +570,7 @@ struct Engine {
     double step_bytes(int st, int T, int nrhs, bool dual_check) const {
         const double M = m, Nn = n, K = k, Tt = T, R = nrhs;
         switch (st) {
-            case S_TOP: return 16;
-            case S_DUALCHECK: return dual_check ? 13 * Nn : 0;
-            case S_CHUZR: return 37 * M + 8 * Tt + 4 * Tt * Tt;
+            case S_CHUZR: return 37 * M + 8 * Tt + 4 * Tt * Tt + (dual_check ? 13 * Nn : 0);
             case S_BTRAN_RHS: return 24.0 * nnz_S + 20 * K;
             case S_BTRAN_GEMV: return 8 * K * K + 8 * K + 12 * M;
             case S_PIVOT_ROW: return 12.0 * ((double)h_rptr[m] - nnz_S) + 8 * K + 4 * Nn + 8 * (Nn - K) + 8 * M + 50 * Nn;
@@ -730,7 +735,7 @@ struct Engine {
 
     // Run the rest of the current iteration from pricing on (after a top event).
     int run_body_once() {
-        pull(); clear_event(); push();
+        pull(); clear_event(); hc->top_done = 1; push();
         if (opt.verbose >= 3) {
             debug_check_representation("before-body");
             dbg_basis.resize(m);
@@ -982,7 +987,7 @@ int ds_create(const ds_options* opts, ds_solver** out) {
     ds_options o;
     ds_default_options(&o);
     if (opts) o = *opts;
-    if (o.refactor_interval < 1 || o.refactor_interval > 240) return DS_ERR_ARG;
+    if (o.refactor_interval < 1 || o.refactor_interval > 200) return DS_ERR_ARG;
     auto* s = new ds_solver{nullptr, ""};
     try {
         s->e = new Engine(o);

@@ -69,6 +69,7 @@ struct Ctl {
     int nflips, prev_q, nrhs, T;
     double dz, obj;
     int cycle, perturbed, need_dual_check, dual_infeas, k;
+    int top_done;               // the host already ran this iteration's loop bookkeeping
     double f_p;                 // phase 1: f[p_idx]
     double z_phase1;            // phase 1 objective (obj_func_val)
     int p1_found, p1_dinf;

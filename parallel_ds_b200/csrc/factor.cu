@@ -41,26 +41,34 @@ __global__ void k_build_K(const int* cptr, const int* crow, const double* cval, 
 // One block.  Pan <- S[:, c0:c0+w]; LU of a working copy over the rows not yet
 // pivoted picks the pivot rows; Winv <- (Pan[pivot rows, :])^-1 by unpivoted
 // Gauss-Jordan (its pivots are the LU's, hence the partial-pivoting choices).
-template <int BS>
-__global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double* Wk, int* rowpiv,
+// SMEM: the working copy (k x w) and the pivoted-row flags live in shared
+// memory (k <= GJ_SMEM_ROWS); otherwise in global memory.
+constexpr int GJ_SMEM_ROWS = 1600;
+template <int BS, bool SMEM>
+__global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double* Wk_g, int* rowpiv,
                            int* piv_rows, double* Winv, int* err) {
+    extern __shared__ double sh[];
     __shared__ double red_v[BS / 32];
     __shared__ int red_i[BS / 32];
     __shared__ int s_r;
     __shared__ double prow[GJ_NB];
     __shared__ double W[GJ_NB][GJ_NB + 1];
     __shared__ double Wi[GJ_NB][GJ_NB + 1];
-    for (int a = 0; a < w; ++a)
-        for (int r = threadIdx.x; r < k; r += BS) {
+    double* Wk = SMEM ? sh : Wk_g;
+    unsigned char* piv = SMEM ? (unsigned char*)(sh + (size_t)k * GJ_NB) : nullptr;
+    for (int r = threadIdx.x; r < k; r += BS) {
+        if (SMEM) piv[r] = rowpiv[r] >= 0 ? 1 : 0;
+        for (int a = 0; a < w; ++a) {
             const double v = S[(size_t)r + (size_t)(c0 + a) * k];
             Pan[(size_t)r + (size_t)a * k] = v;
             Wk[(size_t)r + (size_t)a * k] = v;
         }
+    }
     __syncthreads();
     for (int a = 0; a < w; ++a) {
         double best = -1.0; int bi = -1;
         for (int r = threadIdx.x; r < k; r += BS) {
-            if (rowpiv[r] >= 0) continue;
+            if (SMEM ? piv[r] : (rowpiv[r] >= 0)) continue;
             const double v = fabs(Wk[(size_t)r + (size_t)a * k]);
             if (v > best || (v == best && bi >= 0 && r < bi)) { best = v; bi = r; }
         }
@@ -77,7 +85,10 @@ __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double*
             for (int u = 0; u < BS / 32; ++u)
                 if (red_v[u] > bv || (red_v[u] == bv && red_i[u] >= 0 && (b < 0 || red_i[u] < b))) { bv = red_v[u]; b = red_i[u]; }
             if (b < 0 || !(bv > 1e-300)) { *err = c0 + a + 1; b = -1; }
-            else { rowpiv[b] = c0 + a; piv_rows[c0 + a] = b; }
+            else {
+                rowpiv[b] = c0 + a; piv_rows[c0 + a] = b;
+                if (SMEM) piv[b] = 1;
+            }
             s_r = b;
         }
         __syncthreads();
@@ -87,7 +98,7 @@ __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double*
         __syncthreads();
         const double pv = prow[a];
         for (int r = threadIdx.x; r < k; r += BS) {
-            if (rowpiv[r] >= 0) continue;
+            if (SMEM ? piv[r] : (rowpiv[r] >= 0)) continue;
             const double l = Wk[(size_t)r + (size_t)a * k] / pv;
             if (l != 0.0)
                 for (int b = a + 1; b < w; ++b) Wk[(size_t)r + (size_t)b * k] -= l * prow[b];
@@ -193,9 +204,16 @@ cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s
     k_build_K<<<(k + 255) / 256, 256, 0, s>>>(D.cptr, D.crow, D.cval, F.s_var, F.row_kidx, k, F.S);
     cudaMemsetAsync(F.rowpiv, 0xff, sizeof(int) * k, s);
     cudaMemsetAsync(F.err, 0, sizeof(int), s);
+    const bool smem = k <= GJ_SMEM_ROWS;
+    const size_t psh = smem ? (size_t)k * GJ_NB * sizeof(double) + (size_t)k : 0;
+    if (smem) {
+        cudaError_t e = cudaFuncSetAttribute(k_gj_panel<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psh);
+        if (e != cudaSuccess) return e;
+    }
     for (int c0 = 0; c0 < k; c0 += GJ_NB) {
         const int w = (k - c0 < GJ_NB) ? (k - c0) : GJ_NB;
-        k_gj_panel<256><<<1, 256, 0, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
+        if (smem) k_gj_panel<512, true><<<1, 512, psh, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
+        else k_gj_panel<512, false><<<1, 512, 0, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
         k_gj_rows<<<(k + 127) / 128, 128, 0, s>>>(F.S, k, c0, w, F.piv_rows, F.Winv);
         dim3 g((k + 31) / 32, (k + 31) / 32), b(32, 32);
         k_gj_update<<<g, b, 0, s>>>(F.S, k, c0, w, F.Pan, F.rowpiv, F.piv_rows, F.Winv);

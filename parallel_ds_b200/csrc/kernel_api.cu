@@ -4,6 +4,7 @@
 // inside ds_solve is fed identical input vectors to the reference's routines
 // (DSEPricing, the ratio test with its bound-flipping loop, dotUpdate, the PFI
 // eta file) and its output is compared bit for bit.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -38,7 +39,7 @@ Ctl* new_ctl(Scratch& s) {
     Ctl* c = s.alloc<Ctl>(1);
     Ctl h;
     std::memset(&h, 0, sizeof(h));
-    h.phase = 2; h.ybt_n = -1; h.prev_q = -1; h.max_iter = 1 << 30; h.R = 100;
+    h.phase = 2; h.ybt_n = -1; h.prev_q = -1; h.max_iter = 1 << 30; h.R = 100; h.top_done = 1;
     cudaMemcpy(c, &h, sizeof(Ctl), cudaMemcpyHostToDevice);
     return c;
 }
@@ -71,10 +72,12 @@ int ds_kernel_dse_pricing(int m, int N, const int* basis, const double* x, const
     D.x = s.copy(x, N); D.lb = s.copy(lb, N); D.ub = s.copy(ub, N);
     D.type = s.copy(t8.data(), N);
     D.beta = s.copy(beta, m);
-    D.red = s.alloc<double>(m / 256 + 8); D.redi = s.alloc<int>(2 * (m / 256 + 8));
+    const int nbk = (std::max(m, N - m) + 255) / 256 + 8;
+    D.red = s.alloc<double>(2 * nbk); D.redi = s.alloc<int>(4 * nbk);
     D.ybt = s.alloc<double>(m); D.ybt_pos = s.alloc<int>(D.cap + 1);
     D.eta = s.alloc<double>(1); D.eta_pos = s.alloc<int>(1); D.Mtri = s.alloc<double>(1);
     D.ctl = new_ctl(s);
+    if (init_kernel_attributes(D.cap) != cudaSuccess) return DS_ERR_CUDA;
     if (!D.ctl || !D.ybt) return DS_ERR_CUDA;
     int rc = finish(launch_chuzr_only(D, 0));
     if (rc) return rc;
@@ -119,7 +122,8 @@ int ds_kernel_ratio_test(int n, int N, const int* nonbasis, const double* alpha,
     D.x = s.copy(x, N); D.d = s.copy(d, N); D.lb = s.copy(lb, N); D.ub = s.copy(ub, N);
     D.type = s.copy(t8.data(), N);
     D.theta_arr = s.alloc<double>(n); D.cand = s.alloc<unsigned char>(n);
-    D.redi = s.alloc<int>(n / 256 + 8);
+    D.red = s.alloc<double>(2 * (n / 256 + 8));
+    D.redi = s.alloc<int>(2 * (n / 256 + 8));
     D.ctl = new_ctl(s);
     Ctl h;
     cudaMemcpy(&h, D.ctl, sizeof(Ctl), cudaMemcpyDeviceToHost);
@@ -139,7 +143,7 @@ int ds_kernel_ratio_test(int n, int N, const int* nonbasis, const double* alpha,
 
 int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos, const double* rhs, double* sol,
                         int transpose) {
-    if (m <= 0 || T < 0 || T > 240 || !rhs || !sol || (T > 0 && (!eta || !pos))) return DS_ERR_ARG;
+    if (m <= 0 || T < 0 || T > 200 || !rhs || !sol || (T > 0 && (!eta || !pos))) return DS_ERR_ARG;
     Scratch s;
     Dev D{};
     D.m = m; D.n = 1; D.N = m + 1; D.k = 0; D.cap = T + 1;
@@ -161,6 +165,7 @@ int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos, const d
     double* d_h = s.alloc<double>(D.cap);
     D.y0[0] = d_y0; D.frhs[0] = d_rhs; D.fout[0] = d_out;
     D.ctl = new_ctl(s);
+    if (init_kernel_attributes(D.cap) != cudaSuccess) return DS_ERR_CUDA;
     cudaError_t e = launch_build_mtri(D, T, 0);
     if (e == cudaSuccess) {
         if (!transpose) e = launch_ftran(D, 1, 0, 1, 0);

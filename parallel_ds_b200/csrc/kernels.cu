@@ -4,10 +4,9 @@
 // cudaDualSimplex.cpp:417-648) is this launch sequence, captured once per
 // factor as a CUDA graph:
 //
-//   k_top          loop bookkeeping: iteration++, refactor / restart / perturb
-//   k_dual_check   checkDualFeasible every NEED_RESTART iterations
-//   k_chuzr        CHUZR (DSE pricing + optimality test), then the eta part of
-//                  BTRAN for e_p in the last block
+//   k_chuzr        loop bookkeeping (iteration++, refactor / restart / perturb,
+//                  checkDualFeasible every NEED_RESTART), CHUZR (DSE pricing +
+//                  optimality test), then the eta part of BTRAN for e_p
 //   k_btran_rhs    BTRAN through the basis's slack rows
 //   k_btran_gemv   BTRAN through Kinv^T -> rho
 //   k_pivot_row    alpha_N = rho^T A_N fused with CHUZC part 1; the last block
@@ -119,6 +118,36 @@ __device__ ArgMin block_argmin(ArgMin v) {
     return v;
 }
 
+// The smallest (t, i) pair and the second smallest t value.
+struct Min2 { double t1; int i1; double t2; };
+__device__ __forceinline__ Min2 comb_min2(Min2 a, Min2 b) {
+    if (b.t1 < a.t1 || (b.t1 == a.t1 && b.i1 < a.i1)) return Min2{b.t1, b.i1, fmin(b.t2, a.t1)};
+    return Min2{a.t1, a.i1, fmin(a.t2, b.t1)};
+}
+template <int BS>
+__device__ Min2 block_min2(Min2 v) {
+    __shared__ double s1[BS / 32], s2[BS / 32];
+    __shared__ int si[BS / 32];
+    for (int o = 16; o > 0; o >>= 1) {
+        Min2 u{__shfl_down_sync(0xffffffffu, v.t1, o), __shfl_down_sync(0xffffffffu, v.i1, o),
+               __shfl_down_sync(0xffffffffu, v.t2, o)};
+        v = comb_min2(v, u);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { s1[wid] = v.t1; si[wid] = v.i1; s2[wid] = v.t2; }
+    __syncthreads();
+    if (wid == 0) {
+        v = (lane < BS / 32) ? Min2{s1[lane], si[lane], s2[lane]} : Min2{CUDART_INF, INT_MAX, CUDART_INF};
+        for (int o = 16; o > 0; o >>= 1) {
+            Min2 u{__shfl_down_sync(0xffffffffu, v.t1, o), __shfl_down_sync(0xffffffffu, v.i1, o),
+                   __shfl_down_sync(0xffffffffu, v.t2, o)};
+            v = comb_min2(v, u);
+        }
+    }
+    __syncthreads();
+    return v;   // valid in thread 0
+}
+
 template <int BS>
 __device__ int block_sum_int(int v) {
     __shared__ int s[BS / 32];
@@ -206,18 +235,6 @@ __device__ __forceinline__ bool rt_candidate(double a, unsigned char t, double x
     return t == FREE;
 }
 
-// ======================================================================= top
-__global__ void k_top(Dev D) {
-    Ctl* c = D.ctl;
-    if (threadIdx.x != 0 || halted(c)) return;
-    const int it = ++c->iteration;
-    if (it > c->max_iter) { raise_ev(c, EV_ITER_LIMIT, ST_TOP); return; }
-    if (it % c->R == 0) { raise_ev(c, EV_REFACTOR_DUE, ST_TOP); return; }
-    c->need_dual_check = (it % NEED_RESTART == 0);
-    c->dual_infeas = 0;
-    if (!c->need_dual_check && !c->perturbed && c->cycle > MAX_CYCLE) raise_ev(c, EV_PERTURB, ST_TOP);
-}
-
 // checkDualFeasible over the nonbasic slots; also used standalone (force=1).
 template <int BS>
 __global__ void k_dual_check(Dev D, int force) {
@@ -243,12 +260,22 @@ __global__ void k_dual_check(Dev D, int force) {
 // G[t][u] = eta_u[p_t] - [p_u == p_t] (u < t) couples the product-form factors.
 // FTRAN needs s_t = g_t + sum_{u<t} G[t][u] s_u (s_t is the pivot entry the
 // sequential product form reads before applying eta t); BTRAN needs
-// d_t = h_t + sum_{u>t} G[u][t] d_u.  One warp walks the chain; each step's dot
-// product is spread over the lanes and reduced by shuffles (fixed order).
-__device__ void eta_forward(const Dev& D, const double* g, double* s, int T) {
+// d_t = h_t + sum_{u>t} G[u][t] d_u.  The block first stages G's strict lower
+// triangle in shared memory (packed by rows, row t at t(t-1)/2); then one warp
+// walks the chain, each step's dot product spread over the lanes and reduced by
+// shuffles in a fixed order.
+__device__ __forceinline__ int pk(int t, int u) { return (t * (t - 1)) / 2 + u; }
+
+template <int BS>
+__device__ void stage_G(const Dev& D, double* Gs, int T) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = warp + 1; t < T; t += BS / 32)
+        for (int u = lane; u < t; u += 32) Gs[pk(t, u)] = D.Mtri[(size_t)t * D.cap + u];
+}
+__device__ void eta_forward(const double* Gs, const double* g, double* s, int T) {
     const int lane = threadIdx.x & 31;
     for (int t = 0; t < T; ++t) {
-        const double* Gr = D.Mtri + (size_t)t * D.cap;
+        const double* Gr = Gs + pk(t, 0);
         double v = 0.0;
         for (int u = lane; u < t; u += 32) v += Gr[u] * s[u];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -256,26 +283,40 @@ __device__ void eta_forward(const Dev& D, const double* g, double* s, int T) {
         __syncwarp();
     }
 }
-__device__ void eta_backward(const Dev& D, const double* h, double* dl, int T) {
+__device__ void eta_backward(const double* Gs, const double* h, double* dl, int T) {
     const int lane = threadIdx.x & 31;
     for (int t = T - 1; t >= 0; --t) {
         double v = 0.0;
-        for (int u = t + 1 + lane; u < T; u += 32) v += D.Mtri[(size_t)u * D.cap + t] * dl[u];
+        for (int u = t + 1 + lane; u < T; u += 32) v += Gs[pk(u, t)] * dl[u];
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
         if (lane == 0) dl[t] = h[t] + v;
         __syncwarp();
     }
 }
 
+// y[p_t] += dl[t] for every eta t, duplicates summed in eta order by the thread
+// holding their first occurrence (deterministic, no atomics).
+template <int BS>
+__device__ void scatter_pivots(const Dev& D, double* y, const double* dl, int T) {
+    for (int t = threadIdx.x; t < T; t += BS) {
+        const int pt = D.eta_pos[t];
+        bool first = true;
+        for (int u = 0; u < t; ++u) first &= (D.eta_pos[u] != pt);
+        if (!first) continue;
+        double acc = y[pt];
+        for (int u = t; u < T; ++u) if (D.eta_pos[u] == pt) acc = acc + dl[u];
+        y[pt] = acc;
+    }
+}
+
 // ====================================================================== CHUZR
 // Eta part of BTRAN for the unit vector e_p, run by one block:
-//   h_t = eta_t[p] - [p_t == p],  delta = Mtri^T h,  y = e_p + sum_t delta_t e_{p_t}.
-// (Mtri = (I - G)^-1 with G[t][u] = eta_u[p_t] - [p_u == p_t] for u < t.)
+//   h_t = eta_t[p] - [p_t == p],  d = (I - G^T)^-1 h,  y = e_p + sum_t d_t e_{p_t}.
 template <int BS>
-__device__ void btran_unit_eta(const Dev& D, int p_idx) {
+__device__ void btran_unit_eta(const Dev& D, int p_idx, double* Gs) {
     Ctl* c = D.ctl;
-    __shared__ double h[1024];
-    __shared__ double dl[1024];
+    __shared__ double h[256];
+    __shared__ double dl[256];
     const int T = c->T;
     // clear what the previous BTRAN left in ybt
     const int nprev = c->ybt_n;
@@ -286,73 +327,104 @@ __device__ void btran_unit_eta(const Dev& D, int p_idx) {
     }
     for (int t = threadIdx.x; t < T; t += BS)
         h[t] = D.eta[(size_t)t * D.m + p_idx] - (D.eta_pos[t] == p_idx ? 1.0 : 0.0);
+    stage_G<BS>(D, Gs, T);
     __syncthreads();
-    if (threadIdx.x < 32) eta_backward(D, h, dl, T);
+    if (threadIdx.x < 32) eta_backward(Gs, h, dl, T);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        D.ybt[p_idx] = 1.0;
-        D.ybt_pos[0] = p_idx;
-        for (int t = 0; t < T; ++t) {
-            const int pt = D.eta_pos[t];
-            D.ybt[pt] = D.ybt[pt] + dl[t];
-            D.ybt_pos[t + 1] = pt;
-        }
-        c->ybt_n = T + 1;
-    }
+    if (threadIdx.x == 0) D.ybt[p_idx] = 1.0;
+    for (int t = threadIdx.x; t < T; t += BS) D.ybt_pos[t + 1] = D.eta_pos[t];
+    __syncthreads();
+    scatter_pivots<BS>(D, D.ybt, dl, T);
+    if (threadIdx.x == 0) { D.ybt_pos[0] = p_idx; c->ybt_n = T + 1; }
     __syncthreads();
 }
 
-// DSEPricing (tpp:470-501) + checkPrimalFeasible (tpp:296-324), or phase1Pricing
-// (tpp:746-772) when Ctl::phase == 1.
+// Loop bookkeeping of the reference's while loop (cudaDualSimplex.cpp:419-446:
+// iteration++, refactor every R, dual check every NEED_RESTART, perturbation),
+// then DSEPricing (tpp:470-501) + checkPrimalFeasible (tpp:296-324), or
+// phase1Pricing (tpp:746-772) when Ctl::phase == 1.  Threads cover max(m, n):
+// positions for pricing, nonbasic slots for the dual check.
 template <int BS>
 __global__ void k_chuzr(Dev D) {
+    extern __shared__ double Gs[];
     Ctl* c = D.ctl;
     if (halted(c)) return;
-    const int i = blockIdx.x * BS + threadIdx.x;
     const int phase = c->phase;
+    const bool do_top = (phase == 2 && !c->top_done);
+    int it = c->iteration;
+    int top_ev = EV_NONE;
+    bool dual_chk = false;
+    if (do_top) {
+        it += 1;
+        if (it > c->max_iter) top_ev = EV_ITER_LIMIT;
+        else if (it % c->R == 0) top_ev = EV_REFACTOR_DUE;
+        else {
+            dual_chk = (it % NEED_RESTART == 0);
+            if (!dual_chk && !c->perturbed && c->cycle > MAX_CYCLE) top_ev = EV_PERTURB;
+        }
+    }
+    const int i = blockIdx.x * BS + threadIdx.x;
     ArgMax best{-1.0, INT_MAX};
-    int infeas = 0;
-    if (i < D.m) {
-        const int j = D.basis[i];
-        const unsigned char t = D.type[j];
-        if (phase == 2) {
-            const double x = D.x[j], l = D.lb[j], u = D.ub[j];
-            double dt;
-            if (var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8) {
-                const double w = (dt * dt) / D.beta[i];
-                if (w > 0.0) best = ArgMax{w, i};   // strict '>' against max_weight = 0; NaN never wins
+    int infeas = 0, dbad = 0;
+    if (top_ev == EV_NONE) {
+        if (i < D.m) {
+            const int j = D.basis[i];
+            const unsigned char t = D.type[j];
+            if (phase == 2) {
+                const double x = D.x[j], l = D.lb[j], u = D.ub[j];
+                double dt;
+                if (var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8) {
+                    const double w = (dt * dt) / D.beta[i];
+                    if (w > 0.0) best = ArgMax{w, i};   // strict '>' against max_weight = 0; NaN never wins
+                }
+                infeas = var_primal_ok(t, x, l, u) ? 0 : 1;
+            } else {
+                const double fi = D.f[i];
+                if ((t == LOWER && fi > EPS_F) || (t == UPPER && fi < -EPS_F) || t == BOXED || t == FIXED) {
+                    const double w = (fi * fi) / D.beta[i];
+                    if (w > 0.0 && !D.blocked[j]) best = ArgMax{w, i};
+                }
             }
-            infeas = var_primal_ok(t, x, l, u) ? 0 : 1;
-        } else {
-            const double fi = D.f[i];
-            if ((t == LOWER && fi > EPS_F) || (t == UPPER && fi < -EPS_F) || t == BOXED || t == FIXED) {
-                const double w = (fi * fi) / D.beta[i];
-                if (w > 0.0 && !D.blocked[j]) best = ArgMax{w, i};
-            }
+        }
+        if (dual_chk && i < D.n) {
+            const int j = D.nonbasis[i];
+            dbad = var_dual_bad(D.type[j], D.d[j]) ? 1 : 0;
         }
     }
     best = block_argmax<BS>(best);
     infeas = block_sum_int<BS>(infeas);
+    dbad = block_sum_int<BS>(dbad);
     if (threadIdx.x == 0) {
         D.red[blockIdx.x] = best.w;
         D.redi[blockIdx.x] = best.i;
         D.redi[gridDim.x + blockIdx.x] = infeas;
+        D.redi[2 * gridDim.x + blockIdx.x] = dbad;
     }
     if (!last_block(&c->tickets[2])) return;
     // ---- last block: combine the partials in block order
     __shared__ int s_pidx;
     ArgMax v{-1.0, INT_MAX};
-    int tot = 0;
+    int tot = 0, dtot = 0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
         v = better_max(v, ArgMax{__ldcg(&D.red[b]), __ldcg(&D.redi[b])});
         tot += __ldcg(&D.redi[gridDim.x + b]);
+        dtot += __ldcg(&D.redi[2 * gridDim.x + b]);
     }
     v = block_argmax<BS>(v);
     tot = block_sum_int<BS>(tot);
+    dtot = block_sum_int<BS>(dtot);
     if (threadIdx.x == 0) {
         s_pidx = -1;
+        if (do_top) c->iteration = it;
+        c->top_done = 0;
         const int pidx = (v.i == INT_MAX || v.w <= 0.0) ? -1 : v.i;
-        if (phase == 2) {
+        if (top_ev != EV_NONE) {
+            raise_ev(c, top_ev, ST_TOP);
+        } else if (dual_chk && dtot > 0) {
+            raise_ev(c, EV_DUALINF, ST_TOP);
+        } else if (dual_chk && !c->perturbed && c->cycle > MAX_CYCLE) {
+            raise_ev(c, EV_PERTURB, ST_TOP);
+        } else if (phase == 2) {
             c->primal_feasible = (tot == 0);
             c->p = -1; c->p_idx = -1;
             if (pidx >= 0) {
@@ -386,12 +458,15 @@ __global__ void k_chuzr(Dev D) {
         }
     }
     __syncthreads();
-    if (s_pidx >= 0) btran_unit_eta<BS>(D, s_pidx);
+    if (s_pidx >= 0) btran_unit_eta<BS>(D, s_pidx, Gs);
 }
 
 // Standalone eta part of BTRAN for e_{p_idx} (exact DSE weight recomputation).
 template <int BS>
-__global__ void k_btran_unit(Dev D, int p_idx) { btran_unit_eta<BS>(D, p_idx); }
+__global__ void k_btran_unit(Dev D, int p_idx) {
+    extern __shared__ double Gs[];
+    btran_unit_eta<BS>(D, p_idx, Gs);
+}
 
 // ====================================================================== BTRAN
 // rhs_j = y[s_pos[j]] - sum_{r in col(s_var[j]), r in R} a_rj * y[slackpos(r)]
@@ -547,6 +622,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
     const double sgn_a = (phase == 2) ? (c->is_lower ? -1.0 : 1.0) : (c->f_p > 0 ? -1.0 : 1.0);
     const int i = blockIdx.x * BS + threadIdx.x;
     int ncand = 0;
+    Min2 mm{CUDART_INF, INT_MAX, CUDART_INF};
     if (i < D.n) {
         const int j = D.nonbasis[i];
         double acc = 0.0;
@@ -570,7 +646,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
             if (cand) {
                 ncand = 1;
                 const double tt = dj / a;
-                if (tt < INF_THETA) th = tt;   // NaN and values >= INF are never taken
+                if (tt < INF_THETA) { th = tt; mm = Min2{tt, i, CUDART_INF}; }   // NaN / >= INF never taken
             }
             D.theta_arr[i] = th;
             D.cand[i] = cand ? 1 : 0;
@@ -578,17 +654,31 @@ __global__ void k_pivot_row(Dev D, int mode) {
     }
     ncand = block_sum_int<BS>(ncand);
     if (!(mode & 2)) return;
-    if (threadIdx.x == 0) D.redi[blockIdx.x] = ncand;
+    mm = block_min2<BS>(mm);
+    if (threadIdx.x == 0) {
+        D.redi[blockIdx.x] = ncand;
+        D.redi[gridDim.x + blockIdx.x] = mm.i1;
+        D.red[2 * blockIdx.x] = mm.t1;
+        D.red[2 * blockIdx.x + 1] = mm.t2;
+    }
     if (!last_block(&c->tickets[3])) return;
-    __shared__ int s_tot, s_q;
+    __shared__ int s_tot, s_q, s_fast;
     int tot = 0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += __ldcg(&D.redi[b]);
+    Min2 g{CUDART_INF, INT_MAX, CUDART_INF};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
+        tot += __ldcg(&D.redi[b]);
+        g = comb_min2(g, Min2{__ldcg(&D.red[2 * b]), __ldcg(&D.redi[gridDim.x + b]), __ldcg(&D.red[2 * b + 1])});
+    }
     tot = block_sum_int<BS>(tot);
+    g = block_min2<BS>(g);
     if (threadIdx.x == 0) {
         s_tot = tot;
         c->ncand = tot;
         if (tot == 0) raise_ev(c, phase == 2 ? EV_UNBOUNDED : EV_P1_BLOCK, ST_RATIO);
         else if (phase == 2) c->unbound_checked = 0;
+        // fast path: no second candidate within the tie window of the first
+        // minimiser, so the ordered scan (rt_select) would return it unchanged
+        s_fast = (g.i1 != INT_MAX && g.t2 > g.t1 + RT_WINDOW) ? g.i1 : -1;
     }
     __syncthreads();
     if (s_tot == 0) return;
@@ -596,8 +686,10 @@ __global__ void k_pivot_row(Dev D, int mode) {
     double delta = fabs(c->delta);
     int remaining = s_tot;
     int q_idx = -1;
+    bool first_pass = true;
     while (true) {
-        const int qi = rt_select<BS>(D, sgn_a);
+        const int qi = (first_pass && s_fast >= 0) ? s_fast : rt_select<BS>(D, sgn_a);
+        first_pass = false;
         if (threadIdx.x == 0) s_q = qi;
         __syncthreads();
         if (s_q < 0) break;          // nothing takeable (reference: uninitialised q)
@@ -797,6 +889,7 @@ __global__ void k_ftran_k2(Dev D, int nr_fixed, int force) {
 // last block gathers g_t = y0[p_t] and solves s = Mtri g for the eta chain.
 template <int BS>
 __global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
+    extern __shared__ double Gs[];
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
     const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
@@ -818,16 +911,19 @@ __global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
     __shared__ double sv[MAX_FTRAN_RHS][256];
     for (int t = threadIdx.x; t < T; t += BS)
         for (int q = 0; q < nr; ++q) g[q][t] = __ldcg(&D.y0[q][D.eta_pos[t]]);
+    stage_G<BS>(D, Gs, T);
     __syncthreads();
     const int w = threadIdx.x >> 5;
-    if (w < nr) eta_forward(D, g[w], sv[w], T);
+    if (w < nr) eta_forward(Gs, g[w], sv[w], T);
     __syncthreads();
     for (int t = threadIdx.x; t < T; t += BS)
         for (int q = 0; q < nr; ++q) D.s_eta[q * D.cap + t] = sv[q][t];
 }
 
-// y = y0 + sum_t s_t eta_t (streaming over the eta file); the last block applies
-// the -s_t e_{p_t} terms in eta order and (iteration FTRAN only) the pivot check
+// y = y0 + sum_t s_t eta_t, streaming over the eta file (64-thread blocks so
+// that small m still spreads over many SMs); the last block applies the
+// -s_t e_{p_t} terms (duplicated positions summed in eta order by the thread
+// owning the first occurrence) and, for the iteration FTRAN, the pivot check
 // |alpha_q[p] - alpha_p[q]| > EPS_R (1 + |alpha_q[p]|)  (cudaDualSimplex.cpp:555).
 template <int BS>
 __global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
@@ -841,33 +937,45 @@ __global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
         for (int t = threadIdx.x; t < T; t += BS) s[q][t] = D.s_eta[q * D.cap + t];
     __syncthreads();
     if (i < D.m) {
-        double a0 = D.y0[0][i], a1 = 0.0, a2 = 0.0;
-        if (nr > 1) a1 = D.y0[1][i];
-        if (nr > 2) a2 = D.y0[2][i];
         const double* e = D.eta + i;
-        for (int t = 0; t < T; ++t) {
-            const double ev = e[(size_t)t * D.m];
-            a0 += s[0][t] * ev;
-            if (nr > 1) a1 += s[1][t] * ev;
-            if (nr > 2) a2 += s[2][t] * ev;
+        const size_t M = D.m;
+        if (nr == 1) {
+            double a0 = D.y0[0][i], b0 = 0.0;
+            int t = 0;
+            for (; t + 1 < T; t += 2) { a0 += s[0][t] * e[t * M]; b0 += s[0][t + 1] * e[(t + 1) * M]; }
+            if (t < T) a0 += s[0][t] * e[t * M];
+            D.fout[0][i] = a0 + b0;
+        } else {
+            double a0 = D.y0[0][i], a1 = D.y0[1][i], a2 = (nr > 2) ? D.y0[2][i] : 0.0;
+            for (int t = 0; t < T; ++t) {
+                const double ev = e[t * M];
+                a0 += s[0][t] * ev;
+                a1 += s[1][t] * ev;
+                if (nr > 2) a2 += s[2][t] * ev;
+            }
+            D.fout[0][i] = a0;
+            D.fout[1][i] = a1;
+            if (nr > 2) D.fout[2][i] = a2;
         }
-        D.fout[0][i] = a0;
-        if (nr > 1) D.fout[1][i] = a1;
-        if (nr > 2) D.fout[2][i] = a2;
     }
     if (!last_block(&c->tickets[6])) return;
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < nr; ++q)
-            for (int t = 0; t < T; ++t) {
-                const int pt = D.eta_pos[t];
-                D.fout[q][pt] = __ldcg(&D.fout[q][pt]) - s[q][t];
-            }
-        if (check) {
-            const double aqp = __ldcg(&D.fout[0][c->p_idx]);
-            const double apq = D.alpha[c->q_idx];
-            if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
-            else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
+    for (int t = threadIdx.x; t < T; t += BS) {
+        const int pt = D.eta_pos[t];
+        bool first = true;
+        for (int u = 0; u < t; ++u) first &= (D.eta_pos[u] != pt);
+        if (!first) continue;
+        for (int q = 0; q < nr; ++q) {
+            double acc = __ldcg(&D.fout[q][pt]);
+            for (int u = t; u < T; ++u) if (D.eta_pos[u] == pt) acc = acc - s[q][u];
+            D.fout[q][pt] = acc;
         }
+    }
+    __syncthreads();
+    if (check && threadIdx.x == 0) {
+        const double aqp = __ldcg(&D.fout[0][c->p_idx]);
+        const double apq = D.alpha[c->q_idx];
+        if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
+        else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
     }
 }
 
@@ -1034,18 +1142,46 @@ __global__ void k_eta_dots(Dev D, const double* c0, double* h) {
 // ybt = c0 + sum_t (Mtri^T h)_t e_{p_t}; marks ybt as dense for the next clear.
 template <int BS>
 __global__ void k_btran_dense_fix(Dev D, const double* c0, const double* h) {
-    __shared__ double dl[1024];
+    extern __shared__ double Gs[];
+    __shared__ double dl[256];
+    __shared__ double hs[256];
     const int T = D.ctl->T;
     for (int i = threadIdx.x; i < D.m; i += BS) D.ybt[i] = c0[i];
-    __shared__ double hs[1024];
     for (int t = threadIdx.x; t < T; t += BS) hs[t] = h[t];
+    stage_G<BS>(D, Gs, T);
     __syncthreads();
-    if (threadIdx.x < 32) eta_backward(D, hs, dl, T);
+    if (threadIdx.x < 32) eta_backward(Gs, hs, dl, T);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        for (int t = 0; t < T; ++t) { const int pt = D.eta_pos[t]; D.ybt[pt] = D.ybt[pt] + dl[t]; }
-        D.ctl->ybt_n = -1;
+    scatter_pivots<BS>(D, D.ybt, dl, T);
+    if (threadIdx.x == 0) D.ctl->ybt_n = -1;
+}
+
+// Exact DSE weights right after a refactorisation (no etas): beta_i is the
+// squared norm of row i of B0^-1 (initBetaWeights(false), tpp:53-67, computes
+// the same norms one BTRAN at a time).  Structural position s_pos[j]: row j of
+// Kinv.  Slack position of row r: e_r - (A[r,S] Kinv) on the R' rows.
+template <int BS>
+__global__ void k_beta_exact_struct(Dev D) {
+    const int j = blockIdx.x * BS + threadIdx.x;
+    if (j >= D.k) return;
+    double s = 0.0;
+    for (int t = 0; t < D.k; ++t) { const double v = D.Kinv[(size_t)j + (size_t)t * D.k]; s += v * v; }
+    D.beta[D.s_pos[j]] = s;
+}
+template <int BS>
+__global__ void k_beta_exact_slack(Dev D) {
+    const int r = blockIdx.x;
+    const int sp = D.row_slackpos[r];
+    if (sp < 0) return;
+    const int e0 = D.cpl_ptr[r], e1 = D.cpl_ptr[r + 1];
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < D.k; t += BS) {
+        double v = 0.0;
+        for (int e = e0; e < e1; ++e) v += D.cpl_val[e] * D.Kinv[(size_t)D.cpl_col[e] + (size_t)t * D.k];
+        acc += v * v;
     }
+    acc = block_sum<BS>(acc);
+    if (threadIdx.x == 0) D.beta[sp] = 1.0 + acc;
 }
 
 template <int BS>
@@ -1129,6 +1265,9 @@ __global__ void k_build_mtri(Dev D, int T) {
 
 // ================================================================= launchers
 constexpr int BS = 256;
+constexpr int BS_ETA = 64;   // eta streaming: narrow blocks spread small m over many SMs
+// Shared memory for G's packed lower triangle (eta chains) at capacity cap.
+static size_t g_smem_bytes(int cap) { return sizeof(double) * (size_t)cap * (size_t)(cap - 1) / 2; }
 
 static std::atomic<long long> g_launches{0};
 static thread_local bool g_counting_off = false;
@@ -1138,14 +1277,6 @@ long long launch_count() { return g_launches.load(); }
 static inline int nblk(int n) { return (n + BS - 1) / BS; }
 
 #define LAUNCH_OK() do { cudaError_t e_ = cudaGetLastError(); if (e_ != cudaSuccess) return e_; } while (0)
-
-cudaError_t launch_top(const Dev& D, cudaStream_t s) {
-    k_top<<<1, 32, 0, s>>>(D);
-    k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 0);
-    count_launch(2);
-    LAUNCH_OK();
-    return cudaSuccess;
-}
 
 cudaError_t launch_dual_check(const Dev& D, cudaStream_t s) {
     k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 1);
@@ -1176,23 +1307,32 @@ cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaS
         const size_t sh = (size_t)D.ftr_chunk * MAX_FTRAN_RHS * sizeof(double);
         k_ftran_k2<BS><<<g, BS, sh, s>>>(D, nr_fixed, force);
     }
-    k_ftran_assemble<BS><<<nblk(D.m), BS, 0, s>>>(D, nr_fixed, force);
-    k_eta_apply<BS><<<nblk(D.m), BS, 0, s>>>(D, nr_fixed, check, force);
+    k_ftran_assemble<BS><<<nblk(D.m), BS, g_smem_bytes(D.cap), s>>>(D, nr_fixed, force);
+    k_eta_apply<BS_ETA><<<(D.m + BS_ETA - 1) / BS_ETA, BS_ETA, 0, s>>>(D, nr_fixed, check, force);
     count_launch((D.k > 0 ? 1 : 0) + 2);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 // One kernel of the iteration sequence (profiling launches them one by one).
-const char* const kStepNames[S_NSTEPS] = {"k_top", "k_dual_check", "k_chuzr", "k_btran_rhs", "k_btran_gemv",
-                                          "k_pivot_row", "k_dual_update", "k_ftran_k", "k_ftran_assemble",
-                                          "k_eta_apply", "k_update"};
+const char* const kStepNames[S_NSTEPS] = {"k_chuzr", "k_btran_rhs", "k_btran_gemv", "k_pivot_row",
+                                          "k_dual_update", "k_ftran_k", "k_ftran_assemble", "k_eta_apply",
+                                          "k_update"};
+
+
+cudaError_t init_kernel_attributes(int cap) {
+    const int bytes = (int)g_smem_bytes(cap);
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_chuzr<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_btran_unit<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_ftran_assemble<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_btran_dense_fix<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
 
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
     switch (step) {
-        case S_TOP: k_top<<<1, 32, 0, s>>>(D); break;
-        case S_DUALCHECK: k_dual_check<BS><<<nblk(D.n), BS, 0, s>>>(D, 0); break;
-        case S_CHUZR: k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D); break;
+        case S_CHUZR: k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D); break;
         case S_BTRAN_RHS: if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, 0); else return cudaSuccess; break;
         case S_BTRAN_GEMV: {
             const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
@@ -1210,8 +1350,8 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
                 return cudaSuccess;
             }
             break;
-        case S_FTRAN_ASM: k_ftran_assemble<BS><<<nblk(D.m), BS, 0, s>>>(D, 0, 0); break;
-        case S_ETA_APPLY: k_eta_apply<BS><<<nblk(D.m), BS, 0, s>>>(D, 0, 1, 0); break;
+        case S_FTRAN_ASM: k_ftran_assemble<BS><<<nblk(D.m), BS, g_smem_bytes(D.cap), s>>>(D, 0, 0); break;
+        case S_ETA_APPLY: k_eta_apply<BS_ETA><<<(D.m + BS_ETA - 1) / BS_ETA, BS_ETA, 0, s>>>(D, 0, 1, 0); break;
         case S_UPDATE: k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 0); break;
         default: return cudaErrorInvalidValue;
     }
@@ -1236,7 +1376,7 @@ cudaError_t launch_update_forced(const Dev& D, cudaStream_t s) {
 }
 
 cudaError_t launch_iteration(const Dev& D, cudaStream_t s) {
-    for (int st = S_TOP; st < S_NSTEPS; ++st) {
+    for (int st = S_CHUZR; st < S_NSTEPS; ++st) {
         cudaError_t e = launch_step(D, st, s);
         if (e != cudaSuccess) return e;
     }
@@ -1280,15 +1420,23 @@ cudaError_t launch_reduced_costs(const Dev& D, const double* y, cudaStream_t s) 
 
 cudaError_t launch_btran_dense_eta(const Dev& D, const double* c0, double* h, int T, cudaStream_t s) {
     if (T > 0) k_eta_dots<BS><<<T, BS, 0, s>>>(D, c0, h);
-    k_btran_dense_fix<BS><<<1, BS, 0, s>>>(D, c0, h);
+    k_btran_dense_fix<BS><<<1, BS, g_smem_bytes(D.cap), s>>>(D, c0, h);
     count_launch((T > 0 ? 1 : 0) + 1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_btran_unit(const Dev& D, int p_idx, cudaStream_t s) {
-    k_btran_unit<BS><<<1, BS, 0, s>>>(D, p_idx);
+    k_btran_unit<BS><<<1, BS, g_smem_bytes(D.cap), s>>>(D, p_idx);
     count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_beta_exact(const Dev& D, cudaStream_t s) {
+    if (D.k > 0) k_beta_exact_struct<BS><<<nblk(D.k), BS, 0, s>>>(D);
+    k_beta_exact_slack<128><<<D.m, 128, 0, s>>>(D);
+    count_launch((D.k > 0 ? 1 : 0) + 1);
     LAUNCH_OK();
     return cudaSuccess;
 }
@@ -1315,7 +1463,7 @@ cudaError_t launch_build_mtri(const Dev& D, int T, cudaStream_t s) {
 }
 
 cudaError_t launch_chuzr_only(const Dev& D, cudaStream_t s) {
-    k_chuzr<BS><<<nblk(D.m), BS, 0, s>>>(D);
+    k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D);
     count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;

@@ -21,7 +21,7 @@ struct FactorBufs {
 cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s);
 
 // Kernels of one iteration, in launch order.
-enum Step : int { S_TOP = 0, S_DUALCHECK, S_CHUZR, S_BTRAN_RHS, S_BTRAN_GEMV, S_PIVOT_ROW, S_DUAL_UPDATE,
+enum Step : int { S_CHUZR = 0, S_BTRAN_RHS, S_BTRAN_GEMV, S_PIVOT_ROW, S_DUAL_UPDATE,
                   S_FTRAN_K, S_FTRAN_ASM, S_ETA_APPLY, S_UPDATE, S_NSTEPS };
 extern const char* const kStepNames[S_NSTEPS];
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s);
@@ -31,7 +31,7 @@ void count_launch(int nk);
 void set_launch_counting(bool on);
 long long launch_count();
 
-cudaError_t launch_top(const Dev& D, cudaStream_t s);
+cudaError_t init_kernel_attributes(int cap);
 cudaError_t launch_body(const Dev& D, int from_stage, cudaStream_t s);
 cudaError_t launch_iteration(const Dev& D, cudaStream_t s);
 cudaError_t launch_update_forced(const Dev& D, cudaStream_t s);
@@ -47,6 +47,8 @@ cudaError_t launch_reduced_costs(const Dev& D, const double* y, cudaStream_t s);
 cudaError_t launch_btran_dense_eta(const Dev& D, const double* c0, double* h, int T, cudaStream_t s);
 cudaError_t launch_btran_unit(const Dev& D, int p_idx, cudaStream_t s);
 cudaError_t launch_norm2(const double* v, int n, double* out, cudaStream_t s);
+// Exact DSE weights of B0 (valid with an empty eta file).
+cudaError_t launch_beta_exact(const Dev& D, cudaStream_t s);
 cudaError_t launch_dot_cost_x(const Dev& D, double* out, cudaStream_t s);
 cudaError_t launch_phase1_init(const Dev& D, double* cc, cudaStream_t s);
 

@@ -26,8 +26,9 @@ constexpr int kBlocks = (kMaxSlots + 255) / 256;
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 constexpr size_t kOffCtl = 0;
 constexpr size_t kOffTheta = align256(sizeof(Ctl));
-constexpr size_t kOffRedi = kOffTheta + align256(sizeof(double) * kMaxSlots);
-constexpr size_t kOffCand = kOffRedi + align256(sizeof(int) * (kBlocks + 8));
+constexpr size_t kOffRed = kOffTheta + align256(sizeof(double) * kMaxSlots);
+constexpr size_t kOffRedi = kOffRed + align256(sizeof(double) * 2 * (kBlocks + 8));
+constexpr size_t kOffCand = kOffRedi + align256(sizeof(int) * 2 * (kBlocks + 8));
 constexpr size_t kScratchBytes = kOffCand + align256(kMaxSlots);
 
 // Shared by every call on a device; holds the last call's contents.
@@ -71,7 +72,7 @@ extern "C" int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, c
     // the control block starts from zero every call: tickets, counters, results
     Ctl h;
     std::memset(&h, 0, sizeof(h));
-    h.phase = 2; h.ybt_n = -1; h.prev_q = -1; h.max_iter = 1 << 30; h.R = 100;
+    h.phase = 2; h.ybt_n = -1; h.prev_q = -1; h.max_iter = 1 << 30; h.R = 100; h.top_done = 1;
     h.delta = delta; h.is_lower = is_lower ? 1 : 0;
     Ctl* dctl = (Ctl*)(base + kOffCtl);
     if (cudaMemcpyAsync(dctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s) != cudaSuccess) return DS_ERR_CUDA;
@@ -83,6 +84,7 @@ extern "C" int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, c
     D.x = const_cast<double*>(x); D.d = const_cast<double*>(d);
     D.lb = lb; D.ub = ub; D.type = type;
     D.theta_arr = (double*)(base + kOffTheta);
+    D.red = (double*)(base + kOffRed);
     D.redi = (int*)(base + kOffRedi);
     D.cand = base + kOffCand;
     D.ctl = dctl;
