@@ -98,18 +98,18 @@ def pinned_copy(t):
 def our_arm(args, rank, world, local_rank):
     import numpy as np
     import torch
+    from concurrent.futures import ThreadPoolExecutor
     from parallel_ds_b200 import _lib
     from parallel_ds_b200 import lp as L
     from parallel_ds_b200._lib import DsOptions, DsStats, ptr
 
     torch.cuda.set_device(local_rank)
     lib = _lib.lib()
-    stream = torch.cuda.Stream()
     o = DsOptions()
     lib.ds_default_options(C.byref(o))
     o.device = local_rank
-    o.stream = C.c_void_p(stream.cuda_stream)
     o.pricing = _lib.PRICING_LEARNED if args.pricing == "learned" else _lib.PRICING_DSE
+    Cc = args.concurrency
 
     def new_handle():
         h = C.c_void_p()
@@ -129,27 +129,44 @@ def our_arm(args, rank, world, local_rank):
         lib.ds_get_stats(h, C.byref(s))
         return s
 
+    def solve(h):
+        rc = lib.ds_solve(h)
+        assert rc == 0, lib.ds_last_error(h)
+        return h
+
     K, W = args.steps, args.warmup
-    seeds = [2000 + rank * K + s for s in range(K)]
-    wseeds = [1000 + rank * W + s for s in range(W)]
-    lps = [pinned_copy(L.typed(gen(args.workload, s))) for s in seeds]
-    wlps = [pinned_copy(L.typed(gen(args.workload, s))) for s in wseeds]
+    seeds = [[2000 + (rank * K + s) * Cc + c for c in range(Cc)] for s in range(K)]
+    wseeds = [[1000 + (rank * W + s) * Cc + c for c in range(Cc)] for s in range(W)]
+    lps = [[pinned_copy(L.typed(gen(args.workload, x))) for x in row] for row in seeds]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MB > L2
+    pool = ThreadPoolExecutor(max_workers=Cc)
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
 
-    # warm-up (untimed)
-    for t in wlps:
-        h = new_handle(); load(h, t)
-        assert lib.ds_solve(h) == 0, lib.ds_last_error(h)
-        lib.ds_destroy(h)
+    # warm-up (untimed): same handles and concurrency as the timed steps
+    handles = [new_handle() for _ in range(Cc)]
+    for row in wseeds:
+        ts = [L.typed(gen(args.workload, x)) for x in row]
+        for h, t in zip(handles, ts):
+            load(h, t)
+        list(pool.map(solve, handles))
 
-    # ---- value: LPs resident in HBM, K solves
-    handles = []
-    for t in lps:
-        h = new_handle(); load(h, t); handles.append(h)
+    # single-LP time-to-optimal (one solve alone on the GPU)
+    h1 = new_handle(); load(h1, lps[0][0]); solve(h1)
+    single = {"seed": seeds[0][0], "iterations": stats(h1).iterations, "time_to_optimal_ms": stats(h1).solve_ms,
+              "objective": lib.ds_get_objective(h1), "status": _status(lib.ds_get_status(h1))}
+    roof = profile_roofline(lib, h1)
+    lib.ds_destroy(h1)
+
+    # ---- value: LPs resident in HBM, K steps of Cc concurrent solves
+    step_handles = []
+    for row in lps:
+        hs = [new_handle() for _ in row]
+        for h, t in zip(hs, row):
+            load(h, t)
+        step_handles.append(hs)
     torch.cuda.synchronize()
     clk = Clocks(local_rank) if rank == 0 else None
     if clk:
@@ -157,69 +174,61 @@ def our_arm(args, rank, world, local_rank):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
     barrier(); torch.cuda.synchronize()
     launches0 = lib.ds_kernel_launch_count()
-    iters, statuses = 0, []
-    with torch.cuda.stream(stream):
-        for s, h in enumerate(handles):
-            flush.fill_(float(s))                 # evict the previous step's working set from L2
-            ev[s][0].record(stream)
-            rc = lib.ds_solve(h)
-            ev[s][1].record(stream)
-            assert rc == 0, lib.ds_last_error(h)
-            iters += stats(h).iterations
-            statuses.append(lib.ds_get_status(h))
+    for s, hs in enumerate(step_handles):
+        flush.fill_(float(s))                 # evict the previous step's working set from L2
+        ev[s][0].record()
+        list(pool.map(solve, hs))
+        ev[s][1].record()
     torch.cuda.synchronize(); barrier()
     launches = lib.ds_kernel_launch_count() - launches0
     clocks = clk.stop() if clk else None
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_ms = sum(step_ms)
-    iter_counts = [stats(h).iterations for h in handles]
-    objs = [lib.ds_get_objective(h) for h in handles]
-    solve_stats = [stats(h) for h in handles]
+    allh = [h for hs in step_handles for h in hs]
+    iters = sum(stats(h).iterations for h in allh)
+    statuses = [lib.ds_get_status(h) for h in allh]
+    lp_ms = [stats(h).solve_ms for h in allh]
 
     # ---- e2e: public API from pinned host buffers, H2D + D2H inside the timed region
-    h2d = sum(lp_bytes(t) for t in lps) // K
-    d2h = 8 * (lps[0]["n"] + lps[0]["m"]) + 8 * lps[0]["m"]
-    xs = [np.zeros(t["n"]) for t in lps]
-    ys = [np.zeros(t["m"]) for t in lps]
-    eh = new_handle()
+    h2d = sum(lp_bytes(t) for row in lps for t in row) // (K * Cc) * Cc
+    d2h = (8 * (lps[0][0]["n"] + lps[0][0]["m"]) + 8 * lps[0][0]["m"]) * Cc
+    outs = [(np.zeros(lps[0][0]["n"]), np.zeros(lps[0][0]["m"])) for _ in range(Cc)]
+
+    def e2e_one(args_):
+        h, t, (x, y) = args_
+        load(h, t)
+        solve(h)
+        lib.ds_get_primal(h, ptr(x, C.c_double), None)
+        lib.ds_get_dual(h, ptr(y, C.c_double))
+        return stats(h).iterations
+
     barrier(); torch.cuda.synchronize()
-    e0 = time.perf_counter()
     ee = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    ee[0].record(stream)
-    for s, t in enumerate(lps):
-        load(eh, t)
-        assert lib.ds_solve(eh) == 0
-        lib.ds_get_primal(eh, ptr(xs[s], C.c_double), None)
-        lib.ds_get_dual(eh, ptr(ys[s], C.c_double))
-    ee[1].record(stream)
+    e0 = time.perf_counter()
+    ee[0].record()
+    e_iters = 0
+    for row in lps:
+        e_iters += sum(pool.map(e2e_one, zip(handles, row, outs)))
+    ee[1].record()
     torch.cuda.synchronize(); barrier()
     e_wall_ms = (time.perf_counter() - e0) * 1e3
-    e_ms = ee[0].elapsed_time(ee[1])
-    lib.ds_destroy(eh)
-
-    # ---- roofline of the dominant kernel (replayed on the final state of step 0)
-    roof = None
-    roof = profile_roofline(lib, handles[0])
-
-    for h in handles:
+    e_ms = max(ee[0].elapsed_time(ee[1]), e_wall_ms)
+    for h in allh + handles:
         lib.ds_destroy(h)
+    pool.shutdown()
 
-    # reduce over ranks: max time, summed iterations
     if world > 1:
-        tt = torch.tensor([t_ms, e_ms, e_wall_ms], dtype=torch.float64, device="cuda")
+        tt = torch.tensor([t_ms, e_ms], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        it = torch.tensor([iters], dtype=torch.float64, device="cuda")
+        it = torch.tensor([iters, e_iters], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(it, op=torch.distributed.ReduceOp.SUM)
-        t_ms, e_ms, e_wall_ms = [float(v) for v in tt.tolist()]
-        iters_all = int(it.item())
-    else:
-        iters_all = iters
+        t_ms, e_ms = [float(v) for v in tt.tolist()]
+        iters, e_iters = [int(v) for v in it.tolist()]
     if rank != 0:
         return None
-    e_ms_used = max(e_ms, e_wall_ms)
     res = {
         "metric": METRIC,
-        "value": iters_all / (t_ms / 1e3),
+        "value": iters / (t_ms / 1e3),
         "unit": "iters/s",
         "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": t_ms / K,
@@ -229,16 +238,15 @@ def our_arm(args, rank, world, local_rank):
         "dtype": "f64",
         "data": "synthetic: seeded generator, N(0,1) entries, x0~U[0,1], b=A x0+U[0.1,1], c~U[0,1]",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": args.pricing,
-                   "seeds_rank0": seeds, "refactor_interval": 100, "parallelism": f"replicas x{world}",
-                   "l2": "256 MB buffer written between steps (flush); each step is a full solve",
-                   "step": "one complete solve to optimality"},
-        "time_to_optimal_ms": step_ms,
-        "iterations": iter_counts,
-        "objectives": objs,
-        "statuses": [_status(s) for s in statuses],
-        "refactor_ms": [s.refactor_ms for s in solve_stats],
-        "e2e": {"value": iters_all / (e_ms_used / 1e3), "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms_used / K},
+                   "lps_per_step": Cc, "seeds_rank0": seeds, "refactor_interval": 100,
+                   "parallelism": f"replicas x{world}, {Cc} concurrent solves per GPU",
+                   "l2": "256 MB buffer written between steps (flush); each step solves its LPs to optimality",
+                   "step": f"{Cc} complete solves to optimality, one host thread and CUDA stream each"},
+        "single_lp": single,
+        "lp_time_to_optimal_ms": lp_ms,
+        "statuses": [_status(x) for x in statuses],
+        "e2e": {"value": e_iters / (e_ms / 1e3), "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms / K},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -295,24 +303,25 @@ def reference_arm(args):
     K, W = args.steps, args.warmup
     # bounded sample per step: iteration cap sized so the run ends in a few minutes
     cap = {"plain_small": 10**6, "learned": 4000, "plain_large": 300}[args.workload]
-    lps = [L.typed(gen(args.workload, 2000 + s)) for s in range(K)]
+    nlp = K * args.concurrency
+    lps = [L.typed(gen(args.workload, 2000 + s)) for s in range(nlp)]
     for s in range(min(W, 1)):
         po.solve_typed(L.typed(gen(args.workload, 1000 + s)), max_iterations=min(cap, 200))
     t0 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=min(cores, K)) as ex:
+    with ThreadPoolExecutor(max_workers=min(cores, nlp)) as ex:
         rs = list(ex.map(lambda t: po.solve_typed(t, max_iterations=cap), lps))
     dt = time.perf_counter() - t0
     iters = sum(r["iterations"] for r in rs)
     v = iters / dt
     return {
         "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 0, "steps": K, "warmup": W,
-        "ms_per_step": dt * 1e3 / K * min(cores, K), "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": dt * 1e3 / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "impl": "reference",
         "data": "synthetic: same seeded LPs as the GPU arm",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": "dse",
                    "sample": f"first {cap} iterations of each step's LP"},
-        "cpu_baseline": {"value": v, "unit": "iters/s", "cores": min(cores, K), "kind": "port",
-                         "sample": f"{K} LPs (seeds 2000..{2000 + K - 1}), <= {cap} iterations each, "
+        "cpu_baseline": {"value": v, "unit": "iters/s", "cores": min(cores, nlp), "kind": "port",
+                         "sample": f"{nlp} LPs (seeds 2000..{2000 + nlp - 1}), <= {cap} iterations each, "
                                    f"one LP per host thread"},
         "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "statuses": [r["status"] for r in rs], "iterations": [r["iterations"] for r in rs],
@@ -327,6 +336,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="learned", choices=sorted(WORKLOADS))
     ap.add_argument("--pricing", default="dse", choices=["dse", "learned"])
+    ap.add_argument("--concurrency", type=int, default=8, help="LPs solved at once per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))

@@ -305,7 +305,9 @@ struct Engine {
         // FTRAN launch geometry for this k
         const int tile = 256;
         const int ntile = std::max(1, (k + tile - 1) / tile);
-        int chunk = std::max(64, (k + std::max(1, 296 / ntile) - 1) / std::max(1, 296 / ntile));
+        // about four blocks per SM: chunks of at least 16 rows of Kinv per block
+        const int want = std::max(1, 592 / ntile);
+        int chunk = std::max(16, (k + want - 1) / want);
         const int nchunk = std::max(1, (k + chunk - 1) / chunk);
         D.ftr_tile = tile; D.ftr_chunk = chunk; D.ftr_ntile = ntile; D.ftr_nchunk = nchunk;
         d_part.ensure((size_t)nchunk * MAX_FTRAN_RHS * std::max(k, 1));

@@ -14,6 +14,7 @@
 // No rows are swapped physically; a final gather (k_gj_permute) writes Kinv in
 // natural order.
 #include <cmath>
+#include <mutex>
 
 #include "engine.cuh"
 #include "kernels.cuh"
@@ -58,11 +59,12 @@ __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double*
     unsigned char* piv = SMEM ? (unsigned char*)(sh + (size_t)k * GJ_NB) : nullptr;
     for (int r = threadIdx.x; r < k; r += BS) {
         if (SMEM) piv[r] = rowpiv[r] >= 0 ? 1 : 0;
-        for (int a = 0; a < w; ++a) {
-            const double v = S[(size_t)r + (size_t)(c0 + a) * k];
-            Pan[(size_t)r + (size_t)a * k] = v;
-            Wk[(size_t)r + (size_t)a * k] = v;
-        }
+        double v[GJ_NB];
+#pragma unroll
+        for (int a = 0; a < GJ_NB; ++a) v[a] = (a < w) ? S[(size_t)r + (size_t)(c0 + a) * k] : 0.0;
+#pragma unroll
+        for (int a = 0; a < GJ_NB; ++a)
+            if (a < w) { Pan[(size_t)r + (size_t)a * k] = v[a]; Wk[(size_t)r + (size_t)a * k] = v[a]; }
     }
     __syncthreads();
     for (int a = 0; a < w; ++a) {
@@ -207,8 +209,14 @@ cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s
     const bool smem = k <= GJ_SMEM_ROWS;
     const size_t psh = smem ? (size_t)k * GJ_NB * sizeof(double) + (size_t)k : 0;
     if (smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_gj_panel<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psh);
-        if (e != cudaSuccess) return e;
+        // process-wide attribute: raised once to the largest panel (other threads launch concurrently)
+        static std::once_flag once;
+        static cudaError_t attr = cudaSuccess;
+        std::call_once(once, [] {
+            attr = cudaFuncSetAttribute(k_gj_panel<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)((size_t)GJ_SMEM_ROWS * GJ_NB * sizeof(double) + GJ_SMEM_ROWS));
+        });
+        if (attr != cudaSuccess) return attr;
     }
     for (int c0 = 0; c0 < k; c0 += GJ_NB) {
         const int w = (k - c0 < GJ_NB) ? (k - c0) : GJ_NB;

@@ -27,6 +27,7 @@
 // exactly and the file is compiled with -fmad=false.
 #include <atomic>
 #include <cfloat>
+#include <mutex>
 #include <climits>
 #include <cmath>
 
@@ -268,9 +269,12 @@ __device__ __forceinline__ int pk(int t, int u) { return (t * (t - 1)) / 2 + u; 
 
 template <int BS>
 __device__ void stage_G(const Dev& D, double* Gs, int T) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int t = warp + 1; t < T; t += BS / 32)
-        for (int u = lane; u < t; u += 32) Gs[pk(t, u)] = D.Mtri[(size_t)t * D.cap + u];
+    // one element per thread per row (T <= cap <= 205 < BS); the unrolled row
+    // loop keeps eight independent loads in flight per thread
+    const int u = threadIdx.x;
+#pragma unroll 8
+    for (int t = 1; t < T; ++t)
+        if (u < t) Gs[pk(t, u)] = __ldcg(&D.Mtri[(size_t)t * D.cap + u]);
 }
 __device__ void eta_forward(const double* Gs, const double* g, double* s, int T) {
     const int lane = threadIdx.x & 31;
@@ -853,20 +857,24 @@ __global__ void k_ftran_k2(Dev D, int nr_fixed, int force) {
         double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0;
         const double* col = D.Kinv + (size_t)t0 * k + j;
         const int len = t1 - t0;
+        const int C = D.ftr_chunk;
         if (nr == 1) {
+#pragma unroll 8
             for (int t = 0; t < len; ++t) acc0 += col[(size_t)t * k] * sh[t];
         } else if (nr == 2) {
+#pragma unroll 8
             for (int t = 0; t < len; ++t) {
                 const double kv = col[(size_t)t * k];
                 acc0 += kv * sh[t];
-                acc1 += kv * sh[D.ftr_chunk + t];
+                acc1 += kv * sh[C + t];
             }
         } else {
+#pragma unroll 8
             for (int t = 0; t < len; ++t) {
                 const double kv = col[(size_t)t * k];
                 acc0 += kv * sh[t];
-                acc1 += kv * sh[D.ftr_chunk + t];
-                acc2 += kv * sh[2 * D.ftr_chunk + t];
+                acc1 += kv * sh[C + t];
+                acc2 += kv * sh[2 * C + t];
             }
         }
         double* part = D.ftr_part + (size_t)blockIdx.y * MAX_FTRAN_RHS * k;
@@ -947,6 +955,7 @@ __global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
             D.fout[0][i] = a0 + b0;
         } else {
             double a0 = D.y0[0][i], a1 = D.y0[1][i], a2 = (nr > 2) ? D.y0[2][i] : 0.0;
+#pragma unroll 8
             for (int t = 0; t < T; ++t) {
                 const double ev = e[t * M];
                 a0 += s[0][t] * ev;
@@ -1320,7 +1329,20 @@ const char* const kStepNames[S_NSTEPS] = {"k_chuzr", "k_btran_rhs", "k_btran_gem
                                           "k_update"};
 
 
+static cudaError_t set_kernel_attributes(int cap);
+
+// The dynamic shared memory limits are process-wide function attributes, so
+// they are raised once to the largest size any handle can request (cap 205)
+// rather than per call (solver handles on other threads launch concurrently).
 cudaError_t init_kernel_attributes(int cap) {
+    static std::once_flag once;
+    static cudaError_t result = cudaSuccess;
+    (void)cap;
+    std::call_once(once, [] { result = set_kernel_attributes(205); });
+    return result;
+}
+
+static cudaError_t set_kernel_attributes(int cap) {
     const int bytes = (int)g_smem_bytes(cap);
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(k_chuzr<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
