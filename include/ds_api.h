@@ -66,9 +66,13 @@ typedef struct ds_options {
                                   from std::random_device, baseDualSimplex.tpp:244) */
     int    device;             /* CUDA device ordinal                              */
     void*  stream;             /* cudaStream_t to use, or NULL for an own stream   */
-    double learned_margin;     /* learned pricing: minimum score margin over the
-                                  runner-up before the network's row is taken      */
+    double learned_margin;     /* learned pricing: the network's row is taken only
+                                  when sigmoid(logit) of that row reaches this
+                                  value, else the DSE row is (default 0.5)        */
     int    verbose;            /* 0 silent, 1 events, 2 every iteration            */
+    double learned_mix;        /* learned pricing ranks candidate rows by
+                                  w_i * (mix + (1 - mix) * sigmoid(logit_i)),
+                                  w_i the DSE weight (default 0.05)               */
 } ds_options;
 
 typedef struct ds_stats {
@@ -139,6 +143,49 @@ const char* ds_last_error(const ds_solver* s);
 int ds_set_trace(ds_solver* s, int cap);
 int ds_get_trace(const ds_solver* s, int* p, int* q, double* theta, double* obj, int* count);
 
+
+/* ---- learned pricing ----------------------------------------------------------
+ * No counterpart in the reference (its pricing is DSE only, tpp:470-501).
+ * A model is an MLP DS_NUM_FEATURES -> 64 -> 64 -> 1 (ReLU) whose logit
+ * estimates whether a candidate row's basic variable leaves the basis for good
+ * (is nonbasic at the optimum).  Inference and training run on the tensor
+ * cores (BF16 operands, FP32 accumulation); parameters are FP32 in the order
+ * W1[64][DS_NUM_FEATURES], b1[64], W2[64][64], b2[64], w3[64], b3. */
+#define DS_NUM_FEATURES 12
+#define DS_MLP_NPARAMS (64 * DS_NUM_FEATURES + 64 + 64 * 64 + 64 + 64 + 1)
+/* Features of a candidate row i with basic variable j, at iteration it:
+ *  0 j is a slack            1 log10|delta|/4          2 log10(beta_i)/4
+ *  3 log10(delta^2/beta)/4   4 log10(w_i / w of the previous pick)/4
+ *  5 cost c_j (0 for slacks) 6 nonzeros of column j (slack: of its row)/40
+ *  7 infeasible rows at the previous pricing / m       8 min(it/m, 10)/5
+ *  9 min(times j entered, 20)/5    10 min((it - last entry of j)/m, 5)
+ * 11 sign(x_j) log10(1 + |x_j|)   (logs clamped; see csrc/mlp.cu) */
+typedef struct ds_model ds_model;
+int ds_model_create(int device, ds_model** out);
+int ds_model_destroy(ds_model* m);
+int ds_model_set_params(ds_model* m, const float* params, int count);
+int ds_model_get_params(const ds_model* m, float* params, int count);
+/* Forward pass over rows x DS_NUM_FEATURES floats: logits (rows); H1, H2 (rows x 64
+ * post-ReLU activations, may be NULL). */
+int ds_model_forward(ds_model* m, const float* X, int rows, float* logits, float* H1, float* H2);
+/* Mean binary cross-entropy with logits over the rows and its gradient
+ * (DS_MLP_NPARAMS floats, parameter order). */
+int ds_model_gradients(ds_model* m, const float* X, const float* y, int rows, float* grads, float* loss);
+/* Adam (lr, beta1 0.9, beta2 0.999, eps 1e-8) over epochs of shuffled
+ * mini-batches (batch a multiple of 128); the rows stay on the device.
+ * mean_loss: mean batch loss of the last epoch. */
+int ds_model_train(ds_model* m, const float* X, const float* y, int rows, int epochs, int batch, float lr,
+                   unsigned long long seed, float* mean_loss);
+/* Attach a model (not owned; NULL detaches).  Required when pricing is
+ * DS_PRICING_LEARNED; must live on the solver's device. */
+int ds_set_model(ds_solver* s, ds_model* m);
+/* Feature trace for training: every `every` phase-2 iterations, the features of
+ * each candidate row (up to cap records per solve).  every = 0 turns it off. */
+int ds_set_feature_trace(ds_solver* s, int every, int cap);
+/* feat: count x DS_NUM_FEATURES floats; meta: count x 3 ints (iteration, basis
+ * position, variable), ordered by iteration then position.  *count receives the
+ * number of records kept (at most cap); *total (may be NULL) all candidates seen. */
+int ds_get_feature_trace(const ds_solver* s, float* feat, int* meta, int* count, int* total);
 
 /* Factorise the basis given as m variable indices (structurals 0..n-1, slacks
  * n..n+m-1) and apply B^-1 (transpose = 0: rhs by rows -> out by basis

@@ -17,12 +17,14 @@ STATUS = {0: "unsolved", 1: "optimal", 2: "primal_infeasible", 3: "dual_infeasib
 PRICING_DSE, PRICING_LEARNED = 0, 1
 GEN_DENSITY, GEN_PER_COL, GEN_BLOCK = 0, 1, 2
 NUM_FEATURES = 12
+MLP_NPARAMS = 64 * NUM_FEATURES + 64 + 64 * 64 + 64 + 64 + 1
 
 
 class DsOptions(C.Structure):
     _fields_ = [("refactor_interval", C.c_int), ("max_iterations", C.c_int), ("pricing", C.c_int),
                 ("strict_reference", C.c_int), ("seed", C.c_ulonglong), ("device", C.c_int),
-                ("stream", C.c_void_p), ("learned_margin", C.c_double), ("verbose", C.c_int)]
+                ("stream", C.c_void_p), ("learned_margin", C.c_double), ("verbose", C.c_int),
+                ("learned_mix", C.c_double)]
 
 
 class DsStats(C.Structure):
@@ -81,8 +83,16 @@ def lib():
         "ds_last_error": (C.c_char_p, [C.c_void_p]),
         "ds_set_trace": (C.c_int, [C.c_void_p, C.c_int]),
         "ds_get_trace": (C.c_int, [C.c_void_p, IP, IP, DP, DP, IP]),
-        "ds_set_feature_trace": (C.c_int, [C.c_void_p, C.c_int]),
+        "ds_set_feature_trace": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
         "ds_get_feature_trace": (C.c_int, [C.c_void_p, FP, IP, IP, IP]),
+        "ds_set_model": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "ds_model_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+        "ds_model_destroy": (C.c_int, [C.c_void_p]),
+        "ds_model_set_params": (C.c_int, [C.c_void_p, FP, C.c_int]),
+        "ds_model_get_params": (C.c_int, [C.c_void_p, FP, C.c_int]),
+        "ds_model_forward": (C.c_int, [C.c_void_p, FP, C.c_int, FP, FP, FP]),
+        "ds_model_gradients": (C.c_int, [C.c_void_p, FP, FP, C.c_int, FP, FP]),
+        "ds_model_train": (C.c_int, [C.c_void_p, FP, FP, C.c_int, C.c_int, C.c_int, C.c_float, C.c_ulonglong, FP]),
         "ds_kernel_dse_pricing": (C.c_int, [C.c_int, C.c_int, IP, DP, DP, DP, IP, DP, IP, IP, DP, IP, IP]),
         "ds_kernel_pivot_row": (C.c_int, [C.c_int, C.c_int, IP, IP, DP, IP, DP, DP]),
         "ds_kernel_ratio_test": (C.c_int, [C.c_int, C.c_int, IP, DP, C.c_double, C.c_int, DP, DP, DP, DP,

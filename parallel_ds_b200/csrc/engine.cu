@@ -90,8 +90,8 @@ struct Engine {
     DBuf<unsigned> d_tile_tickets;
     DBuf<double> d_tmp_rows, d_tmp_rows2, d_tmp_pos, d_tmp_pos2, d_h;
     DBuf<Ctl> d_ctl;
-    DBuf<float> d_feat, d_score;
-    DBuf<int> d_row_cnt;
+    DBuf<float> d_score, d_ftr_feat;
+    DBuf<int> d_row_nnz, d_enter_cnt, d_entered_at, d_ftr_meta;
 
     Ctl* hc = nullptr;          // pinned host mirror of Ctl
     Dev D{};
@@ -113,6 +113,11 @@ struct Engine {
     std::vector<int> basis_out;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evr0 = nullptr, evr1 = nullptr;
     MlpModel* mlp = nullptr;    // learned pricing (not owned)
+    int ftr_every = 0, ftr_cap = 0;   // feature trace settings
+    int ftr_total = 0;                // candidates seen by the last traced solve
+    std::vector<float> ftr_feat;      // kept records, sorted by (iteration, position)
+    std::vector<int> ftr_meta;
+    bool model_wait_timeout = false;  // a scoring launch gave up waiting on its MMAs
     long long graph_nodes = 0;  // kernel nodes in the iteration graph
     long long nnz_S = 0, nnz_cpl = 0;   // structural nonzeros in the basis / coupling rows
     // per-kernel profiling (ds_profile_solve)
@@ -208,10 +213,10 @@ struct Engine {
         d_ctl.ensure(1);
         d_Winv.ensure(16 * 16); d_ferr.ensure(1);
         d_trace.ensure(2); d_trace_d.ensure(2);
-        d_feat.ensure((size_t)m * 12); d_score.ensure(m);
+        d_score.ensure(m); d_enter_cnt.ensure(N); d_entered_at.ensure(N);
         std::vector<int> rc(m);
         for (int i = 0; i < m; ++i) rc[i] = h_rptr[i + 1] - h_rptr[i];
-        up(d_row_cnt, rc);
+        up(d_row_nnz, rc);
         CK(cudaMemsetAsync(d_ybt.p, 0, sizeof(double) * m, stream));
         CK(cudaMemsetAsync(d_aq.p, 0, sizeof(double) * m, stream));
         CK(cudaMemsetAsync(d_Mtri.p, 0, sizeof(double) * cap * cap, stream));
@@ -241,7 +246,15 @@ struct Engine {
         D.ftr_part = d_part.p; D.s_eta = d_seta.p; D.red = d_red.p; D.redi = d_redi.p;
         D.flip = d_flip.p; D.flip_list = d_flip_list.p;
         D.trace = d_trace.p; D.trace_d = d_trace_d.p;
-        D.mlp_w = nullptr; D.feat = d_feat.p; D.score = d_score.p; D.feat_row_cnt = d_row_cnt.p;
+        D.learned = (opt.pricing == DS_PRICING_LEARNED && mlp) ? 1 : 0;
+        D.learn_mix = opt.learned_mix;
+        D.learn_margin = opt.learned_margin;
+        D.mlp_w1 = D.mlp_w2 = nullptr; D.mlp_p = nullptr; D.mlp_err = nullptr;
+        if (mlp) model_pointers(mlp, &D.mlp_w1, &D.mlp_w2, &D.mlp_p, &D.mlp_err);
+        D.score = d_score.p; D.row_nnz = d_row_nnz.p;
+        D.enter_count = d_enter_cnt.p; D.entered_at = d_entered_at.p;
+        D.ftr_every = ftr_every; D.ftr_cap = ftr_cap;
+        D.ftr_feat = d_ftr_feat.p; D.ftr_meta = d_ftr_meta.p;
         D.ctl = d_ctl.p;
         D.tile_tickets = d_tile_tickets.p;
     }
@@ -572,6 +585,7 @@ struct Engine {
     double step_bytes(int st, int T, int nrhs, bool dual_check) const {
         const double M = m, Nn = n, K = k, Tt = T, R = nrhs;
         switch (st) {
+            case S_SCORE: return 69 * M + 10248.0 * ((m + 127) / 128);
             case S_CHUZR: return 37 * M + 8 * Tt + 4 * Tt * Tt + (dual_check ? 13 * Nn : 0);
             case S_BTRAN_RHS: return 24.0 * nnz_S + 20 * K;
             case S_BTRAN_GEMV: return 8 * K * K + 8 * K + 12 * M;
@@ -681,6 +695,7 @@ struct Engine {
             bool ran[S_NSTEPS] = {};
             for (int stp = 0; stp < S_NSTEPS; ++stp) {
                 if ((stp == S_BTRAN_RHS || stp == S_FTRAN_K) && k == 0) continue;
+                if (stp == S_SCORE && !score_step_active(D)) continue;
                 CK(cudaEventRecord(pev[2 * stp], stream));
                 CK(launch_step(D, stp, stream));
                 CK(cudaEventRecord(pev[2 * stp + 1], stream));
@@ -861,6 +876,32 @@ struct Engine {
         CK(cudaStreamSynchronize(stream));
     }
 
+    // Copy the feature trace back, ordered by (iteration, position): the device
+    // appends records in completion order.
+    void fetch_feature_trace() {
+        ftr_total = hc->ftr_n;
+        const int kept = std::min(hc->ftr_n, ftr_cap);
+        std::vector<float> f((size_t)kept * DS_NUM_FEATURES);
+        std::vector<int> mt((size_t)kept * 3);
+        if (kept > 0) {
+            CK(cudaMemcpyAsync(f.data(), d_ftr_feat.p, sizeof(float) * f.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaMemcpyAsync(mt.data(), d_ftr_meta.p, sizeof(int) * mt.size(), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+        }
+        std::vector<int> ord(kept);
+        for (int r = 0; r < kept; ++r) ord[r] = r;
+        std::sort(ord.begin(), ord.end(), [&](int a, int b) {
+            if (mt[3 * a] != mt[3 * b]) return mt[3 * a] < mt[3 * b];
+            return mt[3 * a + 1] < mt[3 * b + 1];
+        });
+        ftr_feat.resize(f.size()); ftr_meta.resize(mt.size());
+        for (int r = 0; r < kept; ++r) {
+            std::copy(f.begin() + (size_t)ord[r] * DS_NUM_FEATURES, f.begin() + (size_t)(ord[r] + 1) * DS_NUM_FEATURES,
+                      ftr_feat.begin() + (size_t)r * DS_NUM_FEATURES);
+            std::copy(mt.begin() + 3 * (size_t)ord[r], mt.begin() + 3 * (size_t)(ord[r] + 1), ftr_meta.begin() + 3 * (size_t)r);
+        }
+    }
+
     // presolve + solve + postProcess (tpp:5-30, 123-180) with the cleanup guard
     void solve() {
         if (!loaded) throw CudaError("solve before load", DS_ERR_STATE);
@@ -881,7 +922,18 @@ struct Engine {
         CK(cudaMemsetAsync(d_d.p, 0, sizeof(double) * N, stream));
         CK(cudaMemsetAsync(d_blocked.p, 0, N, stream));
         CK(cudaMemsetAsync(d_aq.p, 0, sizeof(double) * m, stream));
+        CK(cudaMemsetAsync(d_enter_cnt.p, 0, sizeof(int) * N, stream));
+        CK(cudaMemsetAsync(d_entered_at.p, 0, sizeof(int) * N, stream));
         d_trace.alloc(2 * std::max(trace_cap, 1)); d_trace_d.alloc(2 * std::max(trace_cap, 1));
+        if (opt.pricing == DS_PRICING_LEARNED && !mlp)
+            throw CudaError("learned pricing needs a model (ds_set_model)", DS_ERR_STATE);
+        if (mlp && model_device(mlp) != opt.device)
+            throw CudaError("model lives on another device", DS_ERR_STATE);
+        if (ftr_every > 0) {
+            d_ftr_feat.ensure((size_t)ftr_cap * DS_NUM_FEATURES);
+            d_ftr_meta.ensure((size_t)ftr_cap * 3);
+        }
+        invalidate_graph();   // launch parameters may have changed
         std::memset(hc, 0, sizeof(Ctl));
         hc->max_iter = opt.max_iterations; hc->R = std::min(std::max(opt.refactor_interval, 1), cap - 5);
         hc->phase = 2; hc->prev_q = -1; hc->ybt_n = -1; hc->trace_cap = trace_cap;
@@ -929,6 +981,14 @@ struct Engine {
         st.iterations = hc->iteration;
         st.learned_used = hc->learned_used;
         st.learned_fallback = hc->learned_fallback;
+        if (ftr_every > 0) fetch_feature_trace();
+        model_wait_timeout = false;
+        if (D.learned && D.mlp_err) {
+            int fe = 0;
+            CK(cudaMemcpyAsync(&fe, D.mlp_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            model_wait_timeout = fe != 0;
+        }
         x_out.resize(N); d_out.resize(N); basis_out.resize(m);
         CK(cudaMemcpyAsync(x_out.data(), d_x.p, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
         CK(cudaMemcpyAsync(d_out.data(), d_d.p, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
@@ -977,8 +1037,9 @@ void ds_default_options(ds_options* o) {
     o->seed = 12345;
     o->device = 0;
     o->stream = nullptr;
-    o->learned_margin = 0.0;
+    o->learned_margin = 0.5;
     o->verbose = 0;
+    o->learned_mix = 0.05;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }
@@ -1054,6 +1115,9 @@ int ds_solve(ds_solver* s) {
     GUARD(s, {
         s->e->solve();
         if (s->e->status == DS_STATUS_ERROR) return fail(s, DS_ERR_NUMERIC, s->e->err);
+        if (s->e->model_wait_timeout)
+            return fail(s, DS_ERR_DEVICE_WAIT, "a network scoring launch timed out waiting for its MMAs "
+                                               "(those iterations used DSE pricing)");
         return DS_OK;
     })
 }
@@ -1159,6 +1223,32 @@ int ds_get_trace(const ds_solver* s, int* p, int* q, double* theta, double* obj,
         if (obj) obj[t] = e->trace_td[2 * t + 1];
     }
     *count = tn;
+    return DS_OK;
+}
+
+int ds_set_model(ds_solver* s, ds_model* m) {
+    if (!s) return DS_ERR_ARG;
+    s->e->mlp = m ? ds_model_impl(m) : nullptr;
+    s->e->invalidate_graph();
+    return DS_OK;
+}
+
+int ds_set_feature_trace(ds_solver* s, int every, int cap) {
+    if (!s || every < 0 || cap < 0 || (every > 0 && cap == 0)) return DS_ERR_ARG;
+    s->e->ftr_every = every;
+    s->e->ftr_cap = every > 0 ? cap : 0;
+    s->e->invalidate_graph();
+    return DS_OK;
+}
+
+int ds_get_feature_trace(const ds_solver* s, float* feat, int* meta, int* count, int* total) {
+    if (!s || !count) return DS_ERR_ARG;
+    const Engine* e = s->e;
+    const int kept = (int)e->ftr_meta.size() / 3;
+    if (feat) std::copy(e->ftr_feat.begin(), e->ftr_feat.end(), feat);
+    if (meta) std::copy(e->ftr_meta.begin(), e->ftr_meta.end(), meta);
+    *count = kept;
+    if (total) *total = e->ftr_total;
     return DS_OK;
 }
 

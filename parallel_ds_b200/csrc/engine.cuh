@@ -78,6 +78,8 @@ struct Ctl {
     int trace_n, trace_cap;
     int learned_used, learned_fallback;
     int window_fallbacks;       // CHUZC tie-window scans that needed the full scan
+    int ftr_n;                  // feature-trace records written (may exceed the capacity)
+    int ninfeas;                // primal infeasible positions at the last pricing
     int err;
     unsigned tickets[TICKETS];
 };
@@ -124,15 +126,70 @@ struct Dev {
     int* flip_list;     // n
     int* trace;         // 2 * trace_cap ints (p, q)
     double* trace_d;    // 2 * trace_cap doubles (theta, obj)
-    // learned pricing
-    const float* mlp_w;     // packed weights (see mlp.cu)
-    float* feat;            // m * 12 features of the current iteration
-    float* score;           // m scores
-    int* feat_row_cnt;      // m: nonzeros of each row (feature)
+    // learned pricing (mlp.cu)
+    int learned;                // 1: CHUZR ranks rows by DSE weight x network score
+    double learn_mix;           // score = w * (mix + (1 - mix) * sigmoid(logit))
+    double learn_margin;        // minimum sigmoid(logit) of the network's row
+    const void* mlp_w1;         // bf16 W1 (64 x 12), row major
+    const void* mlp_w2;         // bf16 W2 (64 x 64), row major
+    const float* mlp_p;         // fp32 parameters (biases, w3, b3)
+    int* mlp_err;               // set when an MMA completion wait timed out
+    float* score;               // m logits (-inf where the row is not a candidate)
+    int* row_nnz;               // m: nonzeros of each row
+    int* enter_count;           // N: times each variable entered the basis
+    int* entered_at;            // N: iteration of its last entry
+    // feature trace (training data): candidate rows every ftr_every iterations
+    int ftr_every;              // 0: off
+    int ftr_cap;                // records
+    float* ftr_feat;            // ftr_cap x DS_NUM_FEATURES
+    int* ftr_meta;              // ftr_cap x 3: iteration, position, variable
     Ctl* ctl;
     // launch geometry (set per factor)
     int ftr_tile, ftr_chunk, ftr_ntile, ftr_nchunk;
     unsigned* tile_tickets; // ftr_ntile
 };
+
+#ifdef __CUDACC__
+// ------------------------------------------------------------ per-variable rules
+// checkVarIsInfeas (baseDualSimplex.tpp:443-466) with its case fallthrough.
+__device__ __forceinline__ bool var_infeas(unsigned char t, double x, double l, double u, double* delta) {
+    switch (t) {
+        case LOWER:
+            if (x < l - EPS_BOUND) { *delta = x - l; return true; }
+            [[fallthrough]];
+        case UPPER:
+            if (x > u + EPS_BOUND) { *delta = x - u; return true; }
+            [[fallthrough]];
+        case FIXED:
+            if (fabs(x - l) < EPS_BOUND) { *delta = x - l; return true; }
+            [[fallthrough]];
+        case BOXED:
+            if (x > u + EPS_BOUND) { *delta = x - u; return true; }
+            else if (x < l - EPS_BOUND) { *delta = x - l; return true; }
+    }
+    *delta = 0.0;
+    return false;
+}
+
+// checkPrimalFeasible (tpp:296-324) for one basic variable, fallthrough kept.
+__device__ __forceinline__ bool var_primal_ok(unsigned char t, double x, double l, double u) {
+    switch (t) {
+        case FIXED:
+            if (fabs(x - l) > EPS_BOUND) return false;
+            [[fallthrough]];
+        case FREE: return true;
+        case BOXED:
+            if (x > u + EPS_R * fabs(u) + EPS_BOUND || x < l - EPS_R * fabs(l) - EPS_BOUND) return false;
+            [[fallthrough]];
+        case UPPER:
+            if (x > u + EPS_R * fabs(u) + EPS_BOUND) return false;
+            [[fallthrough]];
+        case LOWER:
+            if (x < l - EPS_R * fabs(l) - EPS_BOUND) return false;
+    }
+    return true;
+}
+
+#endif
 
 }  // namespace ds

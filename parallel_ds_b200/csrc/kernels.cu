@@ -180,45 +180,6 @@ __device__ double block_sum(double v) {
 }
 
 // ------------------------------------------------------------ per-variable rules
-// checkVarIsInfeas (baseDualSimplex.tpp:443-466) with its case fallthrough.
-__device__ __forceinline__ bool var_infeas(unsigned char t, double x, double l, double u, double* delta) {
-    switch (t) {
-        case LOWER:
-            if (x < l - EPS_BOUND) { *delta = x - l; return true; }
-            [[fallthrough]];
-        case UPPER:
-            if (x > u + EPS_BOUND) { *delta = x - u; return true; }
-            [[fallthrough]];
-        case FIXED:
-            if (fabs(x - l) < EPS_BOUND) { *delta = x - l; return true; }
-            [[fallthrough]];
-        case BOXED:
-            if (x > u + EPS_BOUND) { *delta = x - u; return true; }
-            else if (x < l - EPS_BOUND) { *delta = x - l; return true; }
-    }
-    *delta = 0.0;
-    return false;
-}
-
-// checkPrimalFeasible (tpp:296-324) for one basic variable, fallthrough kept.
-__device__ __forceinline__ bool var_primal_ok(unsigned char t, double x, double l, double u) {
-    switch (t) {
-        case FIXED:
-            if (fabs(x - l) > EPS_BOUND) return false;
-            [[fallthrough]];
-        case FREE: return true;
-        case BOXED:
-            if (x > u + EPS_R * fabs(u) + EPS_BOUND || x < l - EPS_R * fabs(l) - EPS_BOUND) return false;
-            [[fallthrough]];
-        case UPPER:
-            if (x > u + EPS_R * fabs(u) + EPS_BOUND) return false;
-            [[fallthrough]];
-        case LOWER:
-            if (x < l - EPS_R * fabs(l) - EPS_BOUND) return false;
-    }
-    return true;
-}
-
 // checkDualFeasible (tpp:362-385) for one nonbasic variable.
 __device__ __forceinline__ bool var_dual_bad(unsigned char t, double d) {
     switch (t) {
@@ -368,7 +329,9 @@ __global__ void k_chuzr(Dev D) {
         }
     }
     const int i = blockIdx.x * BS + threadIdx.x;
+    const bool learned = D.learned && phase == 2;
     ArgMax best{-1.0, INT_MAX};
+    ArgMax bestL{-1.0, INT_MAX};   // learned ranking: DSE weight x network score
     int infeas = 0, dbad = 0;
     if (top_ev == EV_NONE) {
         if (i < D.m) {
@@ -379,7 +342,14 @@ __global__ void k_chuzr(Dev D) {
                 double dt;
                 if (var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8) {
                     const double w = (dt * dt) / D.beta[i];
-                    if (w > 0.0) best = ArgMax{w, i};   // strict '>' against max_weight = 0; NaN never wins
+                    if (w > 0.0) {
+                        best = ArgMax{w, i};   // strict '>' against max_weight = 0; NaN never wins
+                        if (learned) {
+                            const double sg = 1.0 / (1.0 + exp(-(double)D.score[i]));
+                            const double v = w * (D.learn_mix + (1.0 - D.learn_mix) * sg);
+                            if (v > 0.0) bestL = ArgMax{v, i};
+                        }
+                    }
                 }
                 infeas = var_primal_ok(t, x, l, u) ? 0 : 1;
             } else {
@@ -396,6 +366,7 @@ __global__ void k_chuzr(Dev D) {
         }
     }
     best = block_argmax<BS>(best);
+    if (learned) bestL = block_argmax<BS>(bestL);
     infeas = block_sum_int<BS>(infeas);
     dbad = block_sum_int<BS>(dbad);
     if (threadIdx.x == 0) {
@@ -403,25 +374,40 @@ __global__ void k_chuzr(Dev D) {
         D.redi[blockIdx.x] = best.i;
         D.redi[gridDim.x + blockIdx.x] = infeas;
         D.redi[2 * gridDim.x + blockIdx.x] = dbad;
+        if (learned) {
+            D.red[gridDim.x + blockIdx.x] = bestL.w;
+            D.redi[3 * gridDim.x + blockIdx.x] = bestL.i;
+        }
     }
     if (!last_block(&c->tickets[2])) return;
     // ---- last block: combine the partials in block order
     __shared__ int s_pidx;
-    ArgMax v{-1.0, INT_MAX};
+    ArgMax v{-1.0, INT_MAX}, vL{-1.0, INT_MAX};
     int tot = 0, dtot = 0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
         v = better_max(v, ArgMax{__ldcg(&D.red[b]), __ldcg(&D.redi[b])});
         tot += __ldcg(&D.redi[gridDim.x + b]);
         dtot += __ldcg(&D.redi[2 * gridDim.x + b]);
+        if (learned) vL = better_max(vL, ArgMax{__ldcg(&D.red[gridDim.x + b]), __ldcg(&D.redi[3 * gridDim.x + b])});
     }
     v = block_argmax<BS>(v);
+    if (learned) vL = block_argmax<BS>(vL);
     tot = block_sum_int<BS>(tot);
     dtot = block_sum_int<BS>(dtot);
     if (threadIdx.x == 0) {
         s_pidx = -1;
         if (do_top) c->iteration = it;
         c->top_done = 0;
-        const int pidx = (v.i == INT_MAX || v.w <= 0.0) ? -1 : v.i;
+        int pidx = (v.i == INT_MAX || v.w <= 0.0) ? -1 : v.i;
+        // Learned pricing: take the network's row when it is a valid leaving
+        // row (a primal infeasible position) whose sigmoid score reaches the
+        // margin; otherwise fall back to the DSE row.
+        if (learned && top_ev == EV_NONE && !(dual_chk && dtot > 0) && pidx >= 0) {
+            const int pl = (vL.i == INT_MAX || !(vL.w > 0.0)) ? -1 : vL.i;
+            const double sg = pl >= 0 ? 1.0 / (1.0 + exp(-(double)D.score[pl])) : 0.0;
+            if (pl >= 0 && sg >= D.learn_margin) { pidx = pl; c->learned_used += 1; }
+            else c->learned_fallback += 1;
+        }
         if (top_ev != EV_NONE) {
             raise_ev(c, top_ev, ST_TOP);
         } else if (dual_chk && dtot > 0) {
@@ -430,6 +416,7 @@ __global__ void k_chuzr(Dev D) {
             raise_ev(c, EV_PERTURB, ST_TOP);
         } else if (phase == 2) {
             c->primal_feasible = (tot == 0);
+            c->ninfeas = tot;
             c->p = -1; c->p_idx = -1;
             if (pidx >= 0) {
                 const int j = D.basis[pidx];
@@ -1041,6 +1028,7 @@ __global__ void k_update(Dev D, int force) {
         D.nonbasis[q_idx] = p;
         D.var_pos[q] = p_idx;
         D.var_pos[p] = -(q_idx + 1);
+        if (D.enter_count) { D.enter_count[q] += 1; D.entered_at[q] = c->iteration; }
         if (phase == 2 && nflips > 0) {
             for (int u = 0; u < D.n; ++u) {
                 const int code = D.flip_list[u];
@@ -1324,7 +1312,7 @@ cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaS
 }
 
 // One kernel of the iteration sequence (profiling launches them one by one).
-const char* const kStepNames[S_NSTEPS] = {"k_chuzr", "k_btran_rhs", "k_btran_gemv", "k_pivot_row",
+const char* const kStepNames[S_NSTEPS] = {"k_mlp_score", "k_chuzr", "k_btran_rhs", "k_btran_gemv", "k_pivot_row",
                                           "k_dual_update", "k_ftran_k", "k_ftran_assemble", "k_eta_apply",
                                           "k_update"};
 
@@ -1354,6 +1342,7 @@ static cudaError_t set_kernel_attributes(int cap) {
 
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
     switch (step) {
+        case S_SCORE: return launch_score(D, s);
         case S_CHUZR: k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D); break;
         case S_BTRAN_RHS: if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, 0); else return cudaSuccess; break;
         case S_BTRAN_GEMV: {
@@ -1382,7 +1371,7 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
 }
 
 cudaError_t launch_body(const Dev& D, int from_stage, cudaStream_t s) {
-    const int first = (from_stage <= ST_PRICING) ? S_CHUZR : S_UPDATE;
+    const int first = (from_stage <= ST_PRICING) ? S_SCORE : S_UPDATE;
     for (int st = first; st < S_NSTEPS; ++st) {
         cudaError_t e = launch_step(D, st, s);
         if (e != cudaSuccess) return e;
@@ -1398,7 +1387,7 @@ cudaError_t launch_update_forced(const Dev& D, cudaStream_t s) {
 }
 
 cudaError_t launch_iteration(const Dev& D, cudaStream_t s) {
-    for (int st = S_CHUZR; st < S_NSTEPS; ++st) {
+    for (int st = S_SCORE; st < S_NSTEPS; ++st) {
         cudaError_t e = launch_step(D, st, s);
         if (e != cudaSuccess) return e;
     }

@@ -21,10 +21,14 @@ struct FactorBufs {
 cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s);
 
 // Kernels of one iteration, in launch order.
-enum Step : int { S_CHUZR = 0, S_BTRAN_RHS, S_BTRAN_GEMV, S_PIVOT_ROW, S_DUAL_UPDATE,
+enum Step : int { S_SCORE = 0, S_CHUZR, S_BTRAN_RHS, S_BTRAN_GEMV, S_PIVOT_ROW, S_DUAL_UPDATE,
                   S_FTRAN_K, S_FTRAN_ASM, S_ETA_APPLY, S_UPDATE, S_NSTEPS };
 extern const char* const kStepNames[S_NSTEPS];
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s);
+// S_SCORE: network scores (learned pricing) and/or the feature trace; no
+// launch when neither is on (mlp.cu).
+bool score_step_active(const Dev& D);
+cudaError_t launch_score(const Dev& D, cudaStream_t s);
 
 // Kernel launch accounting (graph replays are added by the caller).
 void count_launch(int nk);

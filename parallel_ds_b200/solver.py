@@ -115,7 +115,8 @@ class CudaDualSimplex:
     """CudaDualSimplex (cudaDualSimplex.hpp:27-92) backed by libds_b200.so."""
 
     def __init__(self, problem, refactor_interval=100, max_iterations=2000000, pricing="dse",
-                 strict_reference=False, seed=12345, device=0, learned_margin=0.0, model=None):
+                 strict_reference=False, seed=12345, device=0, learned_margin=0.5, learned_mix=0.05,
+                 model=None):
         self.problem = problem
         self.L = _lib.lib()
         o = DsOptions()
@@ -127,6 +128,7 @@ class CudaDualSimplex:
         o.seed = seed
         o.device = device
         o.learned_margin = learned_margin
+        o.learned_mix = learned_mix
         self.opts = o
         self.h = C.c_void_p()
         rc = self.L.ds_create(C.byref(o), C.byref(self.h))
@@ -227,16 +229,37 @@ class CudaDualSimplex:
         del cap
         return dict(p=p, q=q, theta=th, obj=ob)
 
+    def set_feature_trace(self, every, cap):
+        """Record candidate-row features every `every` phase-2 iterations (training data)."""
+        self._check(self.L.ds_set_feature_trace(self.h, int(every), int(cap)), "ds_set_feature_trace")
 
-def solve_lp(lp, **opts):
-    """Solve a generated LP dict (lp.generate) and return a result dict."""
+    def feature_trace(self):
+        """(features [k x 12] float32, meta [k x 3] (iteration, position, variable), total seen)."""
+        cnt, tot = C.c_int(0), C.c_int(0)
+        self._check(self.L.ds_get_feature_trace(self.h, None, None, C.byref(cnt), C.byref(tot)),
+                    "ds_get_feature_trace")
+        k = cnt.value
+        F = np.zeros((k, _lib.NUM_FEATURES), np.float32)
+        M = np.zeros((k, 3), np.int32)
+        self._check(self.L.ds_get_feature_trace(self.h, ptr(F, C.c_float), ptr(M, C.c_int), C.byref(cnt),
+                                                C.byref(tot)), "ds_get_feature_trace")
+        return F, M, tot.value
+
+
+def problem_from_lp(lp):
+    """Problem (reference 8-argument form) of a generated LP dict (lp.generate)."""
     from .lp import typed
     t = typed(lp)
     A = Matrix(t["val"], t["row_ptr"], t["col_idx"], t["m"], t["n"])
     prob = Problem(t["col_type"], t["row_type"], t["c"], t["row_lb"], t["row_ub"], t["col_lb"],
                    t["col_ub"], A)
     prob.transformToComputeForm()
-    s = CudaDualSimplex(prob, **opts)
+    return prob
+
+
+def solve_lp(lp, **opts):
+    """Solve a generated LP dict (lp.generate) and return a result dict."""
+    s = CudaDualSimplex(problem_from_lp(lp), **opts)
     s.initDualSimplex()
     s.presolve("minInfeas")
     sol = s.solve()

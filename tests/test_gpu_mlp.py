@@ -1,0 +1,153 @@
+"""Tensor-core network kernels (csrc/mlp.cu) against the FP64 oracle
+(oracle/mlp_ref.py), and learned pricing inside the solver.
+
+Tolerances (BF16 operands, FP32 accumulation on the GPU; FP64 in the oracle
+with the same BF16 rounding points):
+  per layer, GPU inputs fed to the oracle:  |gpu - ref| <= 1e-4 * (1 + |ref|)
+  end to end (rounding flips can compound):  |z_gpu - z_ref| <= 2e-2 * (1 + |z_ref|)
+  gradient, per parameter block:  ||g_gpu - g_ref|| <= 2e-3 * ||g_ref|| (+1e-7)
+Learned pricing changes only the pivot order: the objective must equal the
+DSE solve's within 1e-9 relative."""
+import numpy as np
+import pytest
+
+from oracle import mlp_ref as R
+from parallel_ds_b200 import learned as LN
+from parallel_ds_b200 import lp as L
+from parallel_ds_b200 import solver as S
+
+pytestmark = pytest.mark.gpu
+
+BLOCKS = dict(W1=(R.OFF_W1, R.OFF_B1), b1=(R.OFF_B1, R.OFF_W2), W2=(R.OFF_W2, R.OFF_B2),
+              b2=(R.OFF_B2, R.OFF_W3), w3=(R.OFF_W3, R.OFF_B3), b3=(R.OFF_B3, R.NPARAMS))
+
+
+def features(rows, seed):
+    """Inputs on the scale of the solver's features (most within [-3, 3])."""
+    r = np.random.default_rng(seed)
+    X = r.normal(0, 1, (rows, R.NF)).astype(np.float32)
+    X[:, 0] = r.random(rows) < 0.5
+    return X
+
+
+def teacher_labels(X):
+    return ((X[:, 3] + 0.5 * X[:, 1] - 0.8 * X[:, 0] + 0.3 * X[:, 5] * X[:, 2]) > 0.1).astype(np.float32)
+
+
+def close(a, b, rtol):
+    return np.all(np.abs(np.asarray(a, np.float64) - b) <= rtol * (1 + np.abs(b)))
+
+
+@pytest.fixture(scope="module")
+def model():
+    return LN.LeavingRowScorer(LN.init_params(3))
+
+
+@pytest.mark.parametrize("rows", [1, 127, 128, 129, 1000])
+def test_forward_matches_oracle(model, rows):
+    X = features(rows, rows)
+    z, H1, H2 = model.forward(X, hidden=True)
+    p = model.params()
+    assert close(H1, R.layer1(p, X), 1e-4)
+    assert close(H2, R.layer2(p, H1), 1e-4)        # layer 2 from the GPU's h1
+    assert close(z, R.head(p, H2), 1e-4)           # head from the GPU's h2
+    assert close(z, R.forward(p, X)[0], 2e-2)      # end to end
+    assert np.all(np.isfinite(z))
+
+
+@pytest.mark.parametrize("rows", [128, 1000, 4096])
+def test_gradients_match_oracle(model, rows):
+    X = features(rows, 100 + rows)
+    y = teacher_labels(X)
+    g, loss = model.gradients(X, y)
+    z, H1, H2 = model.forward(X, hidden=True)
+    p = model.params()
+    gr = R.backward(p, X, y, H1, H2, z)
+    assert abs(loss - R.loss(z, y)) <= 1e-5 * (1 + abs(loss))
+    for name, (a, b) in BLOCKS.items():
+        err = np.linalg.norm(g[a:b] - gr[a:b])
+        assert err <= 2e-3 * np.linalg.norm(gr[a:b]) + 1e-7, (name, err, np.linalg.norm(gr[a:b]))
+    # and against the exact FP64 gradient: BF16 operands cost at most a few percent
+    _, ge = R.loss_and_grad(p, X, y, rounding=False)
+    assert np.linalg.norm(g - ge) <= 5e-2 * np.linalg.norm(ge)
+
+
+def test_training_fits_a_teacher():
+    m = LN.LeavingRowScorer(LN.init_params(5))
+    X = features(32768, 7)
+    y = teacher_labels(X)
+    l0 = R.loss(m.forward(X), y)
+    lt = m.train(X, y, epochs=8, batch=1024, lr=3e-3, seed=1)
+    z1 = m.forward(X)
+    acc = np.mean((z1 > 0) == (y > 0.5))
+    assert lt < 0.5 * l0 and R.loss(z1, y) < 0.25 and acc > 0.9, (l0, lt, acc)
+    # the training step is reproducible: same seed, same parameters
+    m2 = LN.LeavingRowScorer(LN.init_params(5))
+    m2.train(X, y, epochs=8, batch=1024, lr=3e-3, seed=1)
+    np.testing.assert_array_equal(m.params(), m2.params())
+
+
+def test_set_get_params_roundtrip():
+    p = LN.init_params(11)
+    m = LN.LeavingRowScorer(p)
+    np.testing.assert_array_equal(m.params(), p)
+    with pytest.raises(ValueError):
+        m.set_params(p[:-1])
+
+
+def test_feature_trace_records():
+    lp = L.plain_small(seed=2)
+    res, F, y, M = LN.solve_with_trace(lp, every=4, cap=1 << 18)
+    assert res["status"] == "optimal" and len(F) > 0
+    assert res["trace_total"] >= len(F)
+    assert np.all(np.isfinite(F))
+    assert np.all(M[:, 0] % 4 == 0)
+    order = np.lexsort((M[:, 1], M[:, 0]))
+    np.testing.assert_array_equal(order, np.arange(len(M)))
+    n, m = lp["n"], lp["m"]
+    assert np.all((M[:, 1] >= 0) & (M[:, 1] < m)) and np.all((M[:, 2] >= 0) & (M[:, 2] < n + m))
+    np.testing.assert_array_equal(F[:, 0], (M[:, 2] >= n).astype(np.float32))
+    assert set(np.unique(y)) <= {0.0, 1.0}
+
+
+def _solve(lp, trace=0, **kw):
+    s = S.CudaDualSimplex(S.problem_from_lp(lp), **kw)
+    s.initDualSimplex()
+    if trace:
+        s.set_trace(trace)
+    sol = s.solve()
+    return s, sol
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_learned_pricing_keeps_the_optimum(seed):
+    lp = L.plain_small(seed=seed)
+    model = LN.LeavingRowScorer(LN.init_params(seed))
+    s0, sol0 = _solve(lp)
+    s1, sol1 = _solve(lp, pricing="learned", model=model, learned_margin=0.0)
+    assert s0.status() == s1.status() == "optimal"
+    assert abs(sol1.Z - sol0.Z) <= 1e-9 * max(1.0, abs(sol0.Z))
+    assert s1.stats()["learned_used"] > 0
+
+
+def test_learned_pricing_falls_back_to_dse():
+    """margin above any sigmoid value: every pick falls back, so the pivot
+    sequence is the DSE solve's exactly."""
+    lp = L.plain_small(seed=4)
+    model = LN.LeavingRowScorer(LN.init_params(4))
+    s1, sol1 = _solve(lp, trace=1 << 16, pricing="learned", model=model, learned_margin=2.0)
+    s2, sol2 = _solve(lp, trace=1 << 16)
+    st = s1.stats()
+    assert st["learned_used"] == 0 and st["learned_fallback"] > 0
+    t1, t2 = s1.trace(), s2.trace()
+    np.testing.assert_array_equal(t1["p"], t2["p"])
+    np.testing.assert_array_equal(t1["q"], t2["q"])
+    assert sol1.Z == sol2.Z
+
+
+def test_learned_pricing_needs_a_model():
+    lp = L.plain_small(seed=0)
+    s = S.CudaDualSimplex(S.problem_from_lp(lp), pricing="learned")
+    s.initDualSimplex()
+    with pytest.raises(S.DsError):
+        s.solve()
