@@ -73,6 +73,10 @@ typedef struct ds_options {
     double learned_mix;        /* learned pricing ranks candidate rows by
                                   w_i * (mix + (1 - mix) * sigmoid(logit_i)),
                                   w_i the DSE weight (default 0.05)               */
+    int    learned_pdhg_iters; /* learned pricing and feature traces: PDHG
+                                  iterations of the warm-start estimate whose
+                                  bound gaps and duals are network features
+                                  (default 4000; 0 = off)                         */
 } ds_options;
 
 typedef struct ds_stats {
@@ -88,6 +92,7 @@ typedef struct ds_stats {
     int    kernel_launches;    /* kernels launched by the solve                    */
     double solve_ms;           /* device time of ds_solve (CUDA events)            */
     double refactor_ms;        /* device time spent refactorising                  */
+    double pdhg_ms;            /* device time of the PDHG warm-start estimate      */
 } ds_stats;
 
 typedef struct ds_solver ds_solver;
@@ -156,10 +161,13 @@ int ds_get_trace(const ds_solver* s, int* p, int* q, double* theta, double* obj,
 /* Features of a candidate row i with basic variable j, at iteration it:
  *  0 j is a slack            1 log10|delta|/4          2 log10(beta_i)/4
  *  3 log10(delta^2/beta)/4   4 log10(w_i / w of the previous pick)/4
- *  5 cost c_j (0 for slacks) 6 nonzeros of column j (slack: of its row)/40
- *  7 infeasible rows at the previous pricing / m       8 min(it/m, 10)/5
- *  9 min(times j entered, 20)/5    10 min((it - last entry of j)/m, 5)
- * 11 sign(x_j) log10(1 + |x_j|)   (logs clamped; see csrc/mlp.cu) */
+ *  5 asinh(1000 g_j)/8, g_j the distance of the PDHG estimate of j (slack:
+ *    of its row's activity) to its nearest finite bound
+ *  6 asinh(1000 |d_j|)/8, d_j the PDHG estimate's reduced cost of j (slack:
+ *    its row dual)                 7 infeasible rows at the previous pricing / m
+ *  8 min(it/m, 10)/5               9 min(times j entered, 20)/5
+ * 10 min((it - last entry of j)/m, 5)   11 sign(x_j) log10(1 + |x_j|)
+ * (logs and asinh terms clamped; see csrc/mlp.cu) */
 typedef struct ds_model ds_model;
 int ds_model_create(int device, ds_model** out);
 int ds_model_destroy(ds_model* m);
@@ -179,6 +187,11 @@ int ds_model_train(ds_model* m, const float* X, const float* y, int rows, int ep
 /* Attach a model (not owned; NULL detaches).  Required when pricing is
  * DS_PRICING_LEARNED; must live on the solver's device. */
 int ds_set_model(ds_solver* s, ds_model* m);
+/* PDHG estimate of an optimal primal-dual pair of the loaded LP after iters
+ * iterations (rounded up to whole restart periods of 500): x (n), row duals
+ * y (m) with c + A^T y the reduced costs.  The learned scorer's warm-start
+ * evidence, exposed for checking and for callers that want a crash point. */
+int ds_pdhg_estimate(ds_solver* s, int iters, double* x, double* y);
 /* Feature trace for training: every `every` phase-2 iterations, the features of
  * each candidate row (up to cap records per solve).  every = 0 turns it off. */
 int ds_set_feature_trace(ds_solver* s, int every, int cap);

@@ -24,14 +24,15 @@ class DsOptions(C.Structure):
     _fields_ = [("refactor_interval", C.c_int), ("max_iterations", C.c_int), ("pricing", C.c_int),
                 ("strict_reference", C.c_int), ("seed", C.c_ulonglong), ("device", C.c_int),
                 ("stream", C.c_void_p), ("learned_margin", C.c_double), ("verbose", C.c_int),
-                ("learned_mix", C.c_double)]
+                ("learned_mix", C.c_double), ("learned_pdhg_iters", C.c_int)]
 
 
 class DsStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("phase1_iterations", C.c_int), ("refactors", C.c_int),
                 ("restarts", C.c_int), ("perturbed", C.c_int), ("bfrt_flips", C.c_int),
                 ("learned_used", C.c_int), ("learned_fallback", C.c_int), ("bump_size", C.c_int),
-                ("kernel_launches", C.c_int), ("solve_ms", C.c_double), ("refactor_ms", C.c_double)]
+                ("kernel_launches", C.c_int), ("solve_ms", C.c_double), ("refactor_ms", C.c_double),
+                ("pdhg_ms", C.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -86,6 +87,7 @@ def lib():
         "ds_set_feature_trace": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
         "ds_get_feature_trace": (C.c_int, [C.c_void_p, FP, IP, IP, IP]),
         "ds_set_model": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "ds_pdhg_estimate": (C.c_int, [C.c_void_p, C.c_int, DP, DP]),
         "ds_model_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
         "ds_model_destroy": (C.c_int, [C.c_void_p]),
         "ds_model_set_params": (C.c_int, [C.c_void_p, FP, C.c_int]),

@@ -21,6 +21,7 @@
 #include "engine.cuh"
 #include "kernels.cuh"
 #include "mlp.cuh"
+#include "pdhg.cuh"
 
 namespace ds {
 
@@ -91,6 +92,14 @@ struct Engine {
     DBuf<double> d_tmp_rows, d_tmp_rows2, d_tmp_pos, d_tmp_pos2, d_h;
     DBuf<Ctl> d_ctl;
     DBuf<float> d_score, d_ftr_feat;
+    // first-order warm-start evidence (pdhg.cu)
+    DBuf<double> d_pd_c, d_pd_lo, d_pd_hi, d_pd_L, d_pd_U, d_pd_tau, d_pd_sigma;
+    DBuf<double> d_pd_x, d_pd_xbar, d_pd_xsum, d_pd_y, d_pd_ysum;
+    DBuf<float> d_pd_gap, d_pd_dual;
+    PdhgDev PD{};
+    cudaGraphExec_t pd_gexec = nullptr;
+    static constexpr int PDHG_RESTART = 500;
+    cudaEvent_t evp0 = nullptr, evp1 = nullptr;
     DBuf<int> d_row_nnz, d_enter_cnt, d_entered_at, d_ftr_meta;
 
     Ctl* hc = nullptr;          // pinned host mirror of Ctl
@@ -133,12 +142,16 @@ struct Engine {
         else { CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); own_stream = true; }
         CK(cudaMallocHost(&hc, sizeof(Ctl)));
         CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
+        CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
         CK(cudaEventCreate(&evr0)); CK(cudaEventCreate(&evr1));
     }
     ~Engine() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (hc) cudaFreeHost(hc);
         if (ev0) cudaEventDestroy(ev0);
+        if (evp0) cudaEventDestroy(evp0);
+        if (evp1) cudaEventDestroy(evp1);
+        if (pd_gexec) cudaGraphExecDestroy(pd_gexec);
         if (ev1) cudaEventDestroy(ev1);
         if (evr0) cudaEventDestroy(evr0);
         if (evr1) cudaEventDestroy(evr1);
@@ -190,6 +203,7 @@ struct Engine {
             h_type[n + i] = t;
         }
         h_cost_orig = h_cost;
+        setup_pdhg();
         up(d_rptr, h_rptr); up(d_rcol, h_rcol); up(d_rval, h_rval);
         up(d_cptr, h_cptr); up(d_crow, h_crow); up(d_cval, h_cval);
         up(d_lb, h_lb); up(d_ub, h_ub); up(d_cost, h_cost); up(d_type, h_type);
@@ -225,6 +239,70 @@ struct Engine {
         status = DS_STATUS_UNSOLVED;
     }
 
+    // PDHG data of the loaded LP: bounds by variable type (FIXED pins both
+    // sides to lb), row activity bounds from the slack s = -A x, step sizes.
+    void setup_pdhg() {
+        const double inf = INFINITY;
+        auto lower_of = [&](int v) {
+            const int t = h_type[v];
+            return (t == FIXED || t == BOXED || t == LOWER) ? h_lb[v] : -inf;
+        };
+        auto upper_of = [&](int v) {
+            const int t = h_type[v];
+            return t == FIXED ? h_lb[v] : (t == BOXED || t == UPPER) ? h_ub[v] : inf;
+        };
+        std::vector<double> lo(n), hi(n), L(m), U(m), tau(n), sig(m), c(h_cost_orig.begin(), h_cost_orig.begin() + n);
+        for (int j = 0; j < n; ++j) {
+            lo[j] = lower_of(j); hi[j] = upper_of(j);
+            double a = 0;
+            for (int e = h_cptr[j]; e < h_cptr[j + 1]; ++e) a += std::fabs(h_cval[e]);
+            tau[j] = a > 0 ? 1.0 / a : 1.0;
+        }
+        for (int i = 0; i < m; ++i) {
+            L[i] = -upper_of(n + i); U[i] = -lower_of(n + i);
+            double a = 0;
+            for (int e = h_rptr[i]; e < h_rptr[i + 1]; ++e) a += std::fabs(h_rval[e]);
+            sig[i] = a > 0 ? 1.0 / a : 1.0;
+        }
+        up(d_pd_c, c); up(d_pd_lo, lo); up(d_pd_hi, hi); up(d_pd_L, L); up(d_pd_U, U);
+        up(d_pd_tau, tau); up(d_pd_sigma, sig);
+        d_pd_x.ensure(n); d_pd_xbar.ensure(n); d_pd_xsum.ensure(n); d_pd_y.ensure(m); d_pd_ysum.ensure(m);
+        d_pd_gap.ensure(N); d_pd_dual.ensure(N);
+        if (pd_gexec) { cudaGraphExecDestroy(pd_gexec); pd_gexec = nullptr; }
+    }
+
+    // ceil(iters / PDHG_RESTART) restart periods of PDHG from the zero start,
+    // then the per-variable evidence arrays.
+    void run_pdhg(int iters) {
+        PD = PdhgDev{m, n, PDHG_RESTART, d_cptr.p, d_crow.p, d_cval.p, d_rptr.p, d_rcol.p, d_rval.p,
+                     d_pd_c.p, d_pd_lo.p, d_pd_hi.p, d_pd_L.p, d_pd_U.p, d_pd_tau.p, d_pd_sigma.p,
+                     d_pd_x.p, d_pd_xbar.p, d_pd_xsum.p, d_pd_y.p, d_pd_ysum.p};
+        CK(launch_pdhg_init(PD, stream));
+        if (!pd_gexec) {
+            cudaGraph_t g;
+            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            set_launch_counting(false);
+            cudaError_t le = launch_pdhg_period(PD, stream);
+            set_launch_counting(true);
+            cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            CK(le); CK(ce);
+            CK(cudaGraphInstantiate(&pd_gexec, g, 0));
+            cudaGraphDestroy(g);
+        }
+        const int periods = (iters + PDHG_RESTART - 1) / PDHG_RESTART;
+        for (int p = 0; p < periods; ++p) CK(cudaGraphLaunch(pd_gexec, stream));
+        count_launch(periods * 2 * PDHG_RESTART);
+        CK(launch_pdhg_finish(PD, stream));
+        CK(launch_pdhg_evidence(PD, d_pd_gap.p, d_pd_dual.p, stream));
+    }
+
+    void pdhg_estimate(int iters, double* x, double* y) {
+        run_pdhg(iters);
+        CK(cudaMemcpyAsync(x, d_pd_x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(y, d_pd_y.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+    }
+
     void sync_dev() {
         D.m = m; D.n = n; D.N = N; D.cap = cap; D.k = k;
         D.cptr = d_cptr.p; D.crow = d_crow.p; D.cval = d_cval.p;
@@ -255,6 +333,7 @@ struct Engine {
         D.enter_count = d_enter_cnt.p; D.entered_at = d_entered_at.p;
         D.ftr_every = ftr_every; D.ftr_cap = ftr_cap;
         D.ftr_feat = d_ftr_feat.p; D.ftr_meta = d_ftr_meta.p;
+        D.pd_gap = d_pd_gap.p; D.pd_dual = d_pd_dual.p;
         D.ctl = d_ctl.p;
         D.tile_tickets = d_tile_tickets.p;
     }
@@ -934,6 +1013,7 @@ struct Engine {
             d_ftr_meta.ensure((size_t)ftr_cap * 3);
         }
         invalidate_graph();   // launch parameters may have changed
+        const bool want_pd = (opt.pricing == DS_PRICING_LEARNED) || ftr_every > 0;
         std::memset(hc, 0, sizeof(Ctl));
         hc->max_iter = opt.max_iterations; hc->R = std::min(std::max(opt.refactor_interval, 1), cap - 5);
         hc->phase = 2; hc->prev_q = -1; hc->ybt_n = -1; hc->trace_cap = trace_cap;
@@ -941,6 +1021,14 @@ struct Engine {
         push();
         const long long launches0 = launch_count();
         CK(cudaEventRecord(ev0, stream));
+        CK(cudaEventRecord(evp0, stream));
+        if (want_pd && opt.learned_pdhg_iters > 0) {
+            run_pdhg(opt.learned_pdhg_iters);   // warm-start evidence for the scorer's features
+        } else {
+            CK(cudaMemsetAsync(d_pd_gap.p, 0, sizeof(float) * N, stream));
+            CK(cudaMemsetAsync(d_pd_dual.p, 0, sizeof(float) * N, stream));
+        }
+        CK(cudaEventRecord(evp1, stream));
         try {
             refactor();                      // initDualSimplex (cudaDualSimplex.cpp:20-81)
             if (perturb_needed()) perturb();  // presolve (tpp:5-30)
@@ -976,6 +1064,8 @@ struct Engine {
         CK(cudaStreamSynchronize(stream));
         float ms = 0; cudaEventElapsedTime(&ms, ev0, ev1);
         st.solve_ms = ms;
+        float pms = 0; cudaEventElapsedTime(&pms, evp0, evp1);
+        st.pdhg_ms = pms;
         st.kernel_launches = (int)(launch_count() - launches0);
         pull();
         st.iterations = hc->iteration;
@@ -1040,6 +1130,7 @@ void ds_default_options(ds_options* o) {
     o->learned_margin = 0.5;
     o->verbose = 0;
     o->learned_mix = 0.05;
+    o->learned_pdhg_iters = 4000;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }
@@ -1231,6 +1322,15 @@ int ds_set_model(ds_solver* s, ds_model* m) {
     s->e->mlp = m ? ds_model_impl(m) : nullptr;
     s->e->invalidate_graph();
     return DS_OK;
+}
+
+int ds_pdhg_estimate(ds_solver* s, int iters, double* x, double* y) {
+    if (!s || iters <= 0 || !x || !y) return DS_ERR_ARG;
+    if (!s->e->loaded) return fail(s, DS_ERR_STATE, "no LP loaded");
+    GUARD(s, {
+        s->e->pdhg_estimate(iters, x, y);
+        return DS_OK;
+    })
 }
 
 int ds_set_feature_trace(ds_solver* s, int every, int cap) {

@@ -143,6 +143,8 @@ struct Dev {
     int ftr_cap;                // records
     float* ftr_feat;            // ftr_cap x DS_NUM_FEATURES
     int* ftr_meta;              // ftr_cap x 3: iteration, position, variable
+    const float* pd_gap;        // N: PDHG estimate's distance to the nearest bound
+    const float* pd_dual;       // N: PDHG estimate's dual magnitude
     Ctl* ctl;
     // launch geometry (set per factor)
     int ftr_tile, ftr_chunk, ftr_ntile, ftr_nchunk;

@@ -159,8 +159,8 @@ __device__ bool row_features(const Dev& D, int i, int it, float* f) {
     f[2] = clampf(lg10(be), -12, 12) / 4.f;
     f[3] = clampf(lg10(w), -24, 12) / 4.f;
     f[4] = (wl > 0.0 && w > 0.0) ? clampf(lg10(w / wl), -12, 12) / 4.f : 0.f;
-    f[5] = slack ? 0.f : (float)D.cost[j];
-    f[6] = (float)(slack ? D.row_nnz[j - D.n] : (D.cptr[j + 1] - D.cptr[j])) / 40.f;
+    f[5] = clampf(asinh(1000.0 * (double)D.pd_gap[j]) / 8.0, -2, 2);
+    f[6] = clampf(asinh(1000.0 * (double)D.pd_dual[j]) / 8.0, -2, 2);
     f[7] = (float)c->ninfeas / (float)D.m;
     f[8] = clampf((double)it / D.m, 0, 10) / 5.f;
     f[9] = (float)min(D.enter_count[j], 20) / 5.f;

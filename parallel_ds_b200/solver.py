@@ -116,7 +116,7 @@ class CudaDualSimplex:
 
     def __init__(self, problem, refactor_interval=100, max_iterations=2000000, pricing="dse",
                  strict_reference=False, seed=12345, device=0, learned_margin=0.5, learned_mix=0.05,
-                 model=None):
+                 learned_pdhg_iters=4000, model=None):
         self.problem = problem
         self.L = _lib.lib()
         o = DsOptions()
@@ -129,6 +129,7 @@ class CudaDualSimplex:
         o.device = device
         o.learned_margin = learned_margin
         o.learned_mix = learned_mix
+        o.learned_pdhg_iters = learned_pdhg_iters
         self.opts = o
         self.h = C.c_void_p()
         rc = self.L.ds_create(C.byref(o), C.byref(self.h))
@@ -228,6 +229,16 @@ class CudaDualSimplex:
                             ptr(ob, C.c_double), C.byref(cnt))
         del cap
         return dict(p=p, q=q, theta=th, obj=ob)
+
+    def pdhg_estimate(self, iters):
+        """PDHG estimate (x [n], row duals y [m]) of the loaded LP after `iters` iterations."""
+        if not self.loaded:
+            self.initDualSimplex()
+        x = np.zeros(self.problem.A.n)
+        y = np.zeros(self.problem.A.m)
+        self._check(self.L.ds_pdhg_estimate(self.h, int(iters), ptr(x, C.c_double), ptr(y, C.c_double)),
+                    "ds_pdhg_estimate")
+        return x, y
 
     def set_feature_trace(self, every, cap):
         """Record candidate-row features every `every` phase-2 iterations (training data)."""

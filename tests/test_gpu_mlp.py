@@ -151,3 +151,37 @@ def test_learned_pricing_needs_a_model():
     s.initDualSimplex()
     with pytest.raises(S.DsError):
         s.solve()
+
+
+def _mixed_types(lp):
+    """A generated LP with boxed and free columns, equality and >= rows."""
+    t = L.typed(lp)
+    n, m = t["n"], t["m"]
+    ct = t["col_type"].copy(); cub = t["col_ub"].copy(); clb = t["col_lb"].copy()
+    ct[::7] = 2; cub[::7] = 2.0                                  # BOXED [0, 2]
+    rt = t["row_type"].copy(); rlb = t["row_lb"].copy(); rub = t["row_ub"].copy()
+    rt[::11] = 0; rlb[::11] = rub[::11]                          # FIXED rows: equalities
+    rt[5::13] = 4; rlb[5::13] = rub[5::13] - 50.0                # LOWER rows: A x >= b - 50
+    return dict(t, col_type=ct, col_lb=clb, col_ub=cub, row_type=rt, row_lb=rlb, row_ub=rub)
+
+
+@pytest.mark.parametrize("kind", ["plain", "mixed"])
+def test_pdhg_matches_oracle(kind):
+    """GPU PDHG (FP64, warp-order sums) against the numpy restatement over two
+    restart periods: |gpu - ref| <= 1e-8 (1 + |ref|)."""
+    from oracle import pdhg_ref as P
+    lp = L.plain_small(seed=5)
+    t = L.typed(lp) if kind == "plain" else _mixed_types(lp)
+    A = S.Matrix(t["val"], t["row_ptr"], t["col_idx"], t["m"], t["n"])
+    prob = S.Problem(t["col_type"], t["row_type"], t["c"], t["row_lb"], t["row_ub"], t["col_lb"],
+                     t["col_ub"], A)
+    prob.transformToComputeForm()
+    s = S.CudaDualSimplex(prob)
+    s.initDualSimplex()
+    x, y = s.pdhg_estimate(1000)
+    xr, yr = P.pdhg(t, 1000)
+    assert close(x, xr, 1e-8) and close(y, yr, 1e-8)
+    # a second call restarts from the zero start: same result
+    x2, y2 = s.pdhg_estimate(1000)
+    np.testing.assert_array_equal(x, x2)
+    np.testing.assert_array_equal(y, y2)

@@ -40,3 +40,23 @@ def test_bf16_rounding_matches_torch():
     a[:4] = [0.0, -0.0, 1.0 + 2 ** -8, 1.0 + 3 * 2 ** -8]     # exact ties round to even
     ref = torch.tensor(a).to(torch.bfloat16).to(torch.float64).numpy()
     np.testing.assert_array_equal(R.bf16(a), ref)
+
+
+def test_pdhg_restatement_approaches_the_optimum():
+    """The PDHG oracle's estimate on a small generated LP comes close to the
+    HiGHS optimum and identifies most of the optimal basis."""
+    from conftest import highs
+    from oracle import pdhg_ref as P
+    from parallel_ds_b200 import lp as L
+    lp = L.plain_small(seed=3)
+    t = L.typed(lp)
+    r = highs(lp)
+    x, y = P.pdhg(t, 4000)
+    assert abs(lp["c"] @ x - r.fun) <= 1e-2 * abs(r.fun)
+    A = L.to_scipy(lp)
+    slack = lp["b"] - A @ r.x
+    basic = np.concatenate([r.x > 1e-9, slack > 1e-9])
+    pred = np.concatenate([x > 1e-3, y <= 1e-3])
+    assert np.mean(pred == basic) > 0.95
+    gap, dual = P.evidence(t, x, y)
+    assert np.all(np.isfinite(gap)) and np.all(dual >= 0)
