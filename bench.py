@@ -1,17 +1,22 @@
 #!/usr/bin/env python
-"""Benchmark: time-to-optimal and iterations/s of the B200 dual simplex.
+"""Benchmark: time to optimal of the B200 dual simplex, learned vs plain pricing.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload learned|plain_small|plain_large] [--pricing dse|learned]
+                    [--workload learned|plain_small|plain_large] [--pricing learned|dse]
 
-One step = one complete solve (phase 1 + phase 2 to optimality) of one seeded
-LP from the workload's distribution (default: m=2000, n=4000, 1% N(0,1)
-entries, b = A x0 + U[0.1,1], c ~ U[0,1]; held-out seeds 2000+).  Each rank
-solves its own seeds (independent LPs: replicas, weak scaling, no collective in
-the solve).  `value` is total simplex iterations / the max over ranks of the
-summed per-step device time (CUDA events on the solver's stream) with every LP
-already resident in HBM; `e2e` is the same through the public C ABI from pinned
-host buffers (ds_load_typed -> ds_solve -> ds_get_primal / ds_get_dual).
+One step = --concurrency (8) complete solves (phase 1 + phase 2 to an optimal
+status) of seeded LPs from the workload's distribution (default: m=2000,
+n=4000, 1% N(0,1) entries, b = A x0 + U[0.1,1], c ~ U[0,1]; seeds 2000+, never
+used in training), one host thread and CUDA stream per LP.  Each rank solves
+its own seeds (independent LPs: replicas, weak scaling, no collective).
+`value` is LPs solved to optimality per second: solved LPs / the max over
+ranks of the summed per-step device time (CUDA events), every LP already
+resident in HBM.  `time_to_optimal` times --tto-lps of the same LPs solved
+alone on the GPU with the chosen pricing and with plain DSE pricing (same
+seeds, objectives compared).  `e2e` is `value` measured through the public C
+ABI from pinned host buffers (ds_load_typed -> ds_solve -> ds_get_primal /
+ds_get_dual).  `--impl reference` solves the same LPs to optimality with the
+CPU port of the reference's sequential dual simplex on the host cores.
 Rank 0 prints one JSON line.
 """
 import argparse
@@ -100,20 +105,35 @@ def our_arm(args, rank, world, local_rank):
     import torch
     from concurrent.futures import ThreadPoolExecutor
     from parallel_ds_b200 import _lib
+    from parallel_ds_b200 import learned as LN
     from parallel_ds_b200 import lp as L
     from parallel_ds_b200._lib import DsOptions, DsStats, ptr
 
     torch.cuda.set_device(local_rank)
     lib = _lib.lib()
-    o = DsOptions()
-    lib.ds_default_options(C.byref(o))
-    o.device = local_rank
-    o.pricing = _lib.PRICING_LEARNED if args.pricing == "learned" else _lib.PRICING_DSE
     Cc = args.concurrency
+    learned = args.pricing == "learned"
 
-    def new_handle():
+    def options(pricing_learned):
+        o = DsOptions()
+        lib.ds_default_options(C.byref(o))
+        o.device = local_rank
+        o.pricing = _lib.PRICING_LEARNED if pricing_learned else _lib.PRICING_DSE
+        return o
+
+    model = C.c_void_p()
+    if learned:
+        with np.load(args.weights) as f:
+            params = np.ascontiguousarray(f["params"], dtype=np.float32)
+        assert lib.ds_model_create(local_rank, C.byref(model)) == 0
+        assert lib.ds_model_set_params(model, ptr(params, C.c_float), len(params)) == 0
+
+    def new_handle(pricing_learned=learned):
         h = C.c_void_p()
+        o = options(pricing_learned)
         assert lib.ds_create(C.byref(o), C.byref(h)) == 0
+        if pricing_learned:
+            assert lib.ds_set_model(h, model) == 0
         return h
 
     def load(h, t):
@@ -145,20 +165,42 @@ def our_arm(args, rank, world, local_rank):
         if world > 1:
             torch.distributed.barrier()
 
-    # warm-up (untimed): same handles and concurrency as the timed steps
+    # warm-up (untimed): same handles and concurrency as the timed steps, and one plain solve
     handles = [new_handle() for _ in range(Cc)]
     for row in wseeds:
         ts = [L.typed(gen(args.workload, x)) for x in row]
         for h, t in zip(handles, ts):
             load(h, t)
         list(pool.map(solve, handles))
+    hp = new_handle(False)
+    load(hp, L.typed(gen(args.workload, 999)))
+    solve(hp)
 
-    # single-LP time-to-optimal (one solve alone on the GPU)
-    h1 = new_handle(); load(h1, lps[0][0]); solve(h1)
-    single = {"seed": seeds[0][0], "iterations": stats(h1).iterations, "time_to_optimal_ms": stats(h1).solve_ms,
-              "objective": lib.ds_get_objective(h1), "status": _status(lib.ds_get_status(h1))}
+    # ---- time to optimal, one LP alone on the GPU: learned vs plain on the same seeds
+    tto = []
+    h1 = new_handle()
+    for t in [lp for row in lps for lp in row][:args.tto_lps]:
+        load(h1, t); solve(h1)
+        a = dict(ms=stats(h1).solve_ms, it=stats(h1).iterations, obj=lib.ds_get_objective(h1),
+                 st=_status(lib.ds_get_status(h1)), pdhg_ms=stats(h1).pdhg_ms)
+        load(hp, t); solve(hp)
+        b = dict(ms=stats(hp).solve_ms, it=stats(hp).iterations, obj=lib.ds_get_objective(hp),
+                 st=_status(lib.ds_get_status(hp)))
+        tto.append((a, b))
     roof = profile_roofline(lib, h1)
     lib.ds_destroy(h1)
+    tto_block = None
+    if tto:
+        ta, tb = sum(a["ms"] for a, _ in tto), sum(b["ms"] for _, b in tto)
+        tto_block = {
+            "lps": len(tto), "pricing": args.pricing,
+            "ms": [a["ms"] for a, _ in tto], "plain_ms": [b["ms"] for _, b in tto],
+            "iterations": [a["it"] for a, _ in tto], "plain_iterations": [b["it"] for _, b in tto],
+            "mean_ms": ta / len(tto), "plain_mean_ms": tb / len(tto), "speedup_vs_plain": tb / ta,
+            "pdhg_ms": [a.get("pdhg_ms", 0.0) for a, _ in tto],
+            "max_obj_rel_err_vs_plain": max(abs(a["obj"] - b["obj"]) / max(1.0, abs(b["obj"])) for a, b in tto),
+            "statuses": sorted({a["st"] for a, _ in tto} | {b["st"] for _, b in tto}),
+        }
 
     # ---- value: LPs resident in HBM, K steps of Cc concurrent solves
     step_handles = []
@@ -188,6 +230,7 @@ def our_arm(args, rank, world, local_rank):
     iters = sum(stats(h).iterations for h in allh)
     statuses = [lib.ds_get_status(h) for h in allh]
     lp_ms = [stats(h).solve_ms for h in allh]
+    n_solved = sum(1 for x in statuses if x == 1)
 
     # ---- e2e: public API from pinned host buffers, H2D + D2H inside the timed region
     h2d = sum(lp_bytes(t) for row in lps for t in row) // (K * Cc) * Cc
@@ -200,36 +243,38 @@ def our_arm(args, rank, world, local_rank):
         solve(h)
         lib.ds_get_primal(h, ptr(x, C.c_double), None)
         lib.ds_get_dual(h, ptr(y, C.c_double))
-        return stats(h).iterations
+        return 1 if lib.ds_get_status(h) == 1 else 0
 
     barrier(); torch.cuda.synchronize()
     ee = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
     e0 = time.perf_counter()
     ee[0].record()
-    e_iters = 0
+    e_solved = 0
     for row in lps:
-        e_iters += sum(pool.map(e2e_one, zip(handles, row, outs)))
+        e_solved += sum(pool.map(e2e_one, zip(handles, row, outs)))
     ee[1].record()
     torch.cuda.synchronize(); barrier()
     e_wall_ms = (time.perf_counter() - e0) * 1e3
     e_ms = max(ee[0].elapsed_time(ee[1]), e_wall_ms)
-    for h in allh + handles:
+    for h in allh + handles + [hp]:
         lib.ds_destroy(h)
+    if learned:
+        lib.ds_model_destroy(model)
     pool.shutdown()
 
     if world > 1:
         tt = torch.tensor([t_ms, e_ms], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        it = torch.tensor([iters, e_iters], dtype=torch.float64, device="cuda")
+        it = torch.tensor([iters, n_solved, e_solved], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(it, op=torch.distributed.ReduceOp.SUM)
         t_ms, e_ms = [float(v) for v in tt.tolist()]
-        iters, e_iters = [int(v) for v in it.tolist()]
+        iters, n_solved, e_solved = [int(v) for v in it.tolist()]
     if rank != 0:
         return None
     res = {
         "metric": METRIC,
-        "value": iters / (t_ms / 1e3),
-        "unit": "iters/s",
+        "value": n_solved / (t_ms / 1e3),
+        "unit": "LPs/s",
         "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": t_ms / K,
         "higher_is_better": True,
@@ -238,14 +283,18 @@ def our_arm(args, rank, world, local_rank):
         "dtype": "f64",
         "data": "synthetic: seeded generator, N(0,1) entries, x0~U[0,1], b=A x0+U[0.1,1], c~U[0,1]",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": args.pricing,
+                   "scorer": os.path.relpath(args.weights, ROOT) if learned else None,
                    "lps_per_step": Cc, "seeds_rank0": seeds, "refactor_interval": 100,
                    "parallelism": f"replicas x{world}, {Cc} concurrent solves per GPU",
                    "l2": "256 MB buffer written between steps (flush); each step solves its LPs to optimality",
-                   "step": f"{Cc} complete solves to optimality, one host thread and CUDA stream each"},
-        "single_lp": single,
+                   "step": f"{Cc} complete solves to optimality (status optimal), one host thread and CUDA "
+                           f"stream each"},
+        "iters_per_s": iters / (t_ms / 1e3),
+        "iterations": iters,
+        "time_to_optimal": tto_block,
         "lp_time_to_optimal_ms": lp_ms,
-        "statuses": [_status(x) for x in statuses],
-        "e2e": {"value": e_iters / (e_ms / 1e3), "unit": "iters/s", "h2d_bytes_per_step": int(h2d),
+        "statuses": sorted({_status(x) for x in statuses}),
+        "e2e": {"value": e_solved / (e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms / K},
         "gpu_launches": int(launches),
         "clocks": clocks,
@@ -277,68 +326,96 @@ def profile_roofline(lib, h):
             "kernels": prof["kernels"]}
 
 
-def cpu_sample(workload, seconds=15.0, threads=1):
-    """The oracle (CPU port of the reference) on a bounded sample of the workload."""
+def cpu_sample(workload):
+    """The oracle (CPU port of the reference) solving one LP of the workload to
+    optimality on one host core."""
     from oracle import pyoracle as po
     from parallel_ds_b200 import lp as L
     t = L.typed(gen(workload, 2000))
-    # size the iteration cap from a short probe so the sample takes ~`seconds`
     t0 = time.perf_counter()
-    r = po.solve_typed(t, max_iterations=200)
+    r = po.solve_typed(t)
     dt = time.perf_counter() - t0
-    cap = int(max(200, min(200 * seconds / max(dt, 1e-3) * 0.6, 1e6)))
-    t0 = time.perf_counter()
-    r = po.solve_typed(t, max_iterations=cap)
-    dt = time.perf_counter() - t0
-    return {"value": r["iterations"] / dt, "unit": "iters/s", "cores": threads, "kind": "port",
-            "sample": f"oracle on seed 2000, first {r['iterations']} iterations ({r['status']}), {dt:.1f} s"}
+    return {"value": 1.0 / dt, "unit": "LPs/s", "cores": 1, "kind": "port",
+            "sample": f"oracle solves seed 2000 to {r['status']} in {r['iterations']} iterations, {dt:.1f} s "
+                      f"({r['iterations'] / dt:.0f} iterations/s)"}
 
 
 def reference_arm(args):
-    """The reference's CPU algorithm (oracle port) on the host cores, one LP per thread."""
+    """The reference's CPU algorithm (the oracle port: sequential dual simplex
+    with DSE pricing) solving the GPU arm's LPs to optimality, one LP per host
+    thread on all host cores."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import pyoracle as po
     from parallel_ds_b200 import lp as L
     cores = os.cpu_count() or 1
     K, W = args.steps, args.warmup
-    # bounded sample per step: iteration cap sized so the run ends in a few minutes
-    cap = {"plain_small": 10**6, "learned": 4000, "plain_large": 300}[args.workload]
-    nlp = K * args.concurrency
-    lps = [L.typed(gen(args.workload, 2000 + s)) for s in range(nlp)]
-    for s in range(min(W, 1)):
-        po.solve_typed(L.typed(gen(args.workload, 1000 + s)), max_iterations=min(cap, 200))
+    per_step = max(1, min(args.concurrency, cores))
+    lps = [[L.typed(gen(args.workload, 2000 + s * args.concurrency + c)) for c in range(per_step)]
+           for s in range(K)]
+    po.solve_typed(L.typed(gen("plain_small", 1000)))      # warm-up: load the library, fault in pages
+    rs = []
     t0 = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=min(cores, nlp)) as ex:
-        rs = list(ex.map(lambda t: po.solve_typed(t, max_iterations=cap), lps))
+    with ThreadPoolExecutor(max_workers=per_step) as ex:
+        for row in lps:
+            rs += list(ex.map(po.solve_typed, row))
     dt = time.perf_counter() - t0
-    iters = sum(r["iterations"] for r in rs)
-    v = iters / dt
+    solved = sum(1 for r in rs if r["status"] == "optimal")
+    v = solved / dt
     return {
-        "metric": METRIC, "value": v, "unit": "iters/s", "n_gpus": 0, "steps": K, "warmup": W,
+        "metric": METRIC, "value": v, "unit": "LPs/s", "n_gpus": 0, "steps": K, "warmup": W,
         "ms_per_step": dt * 1e3 / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "impl": "reference",
-        "data": "synthetic: same seeded LPs as the GPU arm",
+        "data": "synthetic: the GPU arm's seeded LPs",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": "dse",
-                   "sample": f"first {cap} iterations of each step's LP"},
-        "cpu_baseline": {"value": v, "unit": "iters/s", "cores": min(cores, nlp), "kind": "port",
-                         "sample": f"{nlp} LPs (seeds 2000..{2000 + nlp - 1}), <= {cap} iterations each, "
-                                   f"one LP per host thread"},
-        "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "statuses": [r["status"] for r in rs], "iterations": [r["iterations"] for r in rs],
+                   "step": f"{per_step} LPs solved to optimality, one per host thread"},
+        "cpu_baseline": {"value": v, "unit": "LPs/s", "cores": per_step, "kind": "port",
+                         "sample": f"{len(rs)} LPs (seeds of the GPU arm's steps) solved to optimality, "
+                                   f"{sum(r['iterations'] for r in rs)} iterations, {dt:.1f} s"},
+        "e2e": {"value": v, "unit": "LPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "iters_per_s": sum(r["iterations"] for r in rs) / dt,
+        "statuses": sorted({r["status"] for r in rs}),
     }
+
+
+def solve_one(args):
+    """One LP of the workload (seed --solve-one) solved alone, stats as JSON:
+    the small, fixed command that profiler captures run."""
+    import numpy as np
+    from parallel_ds_b200 import learned as LN
+    from parallel_ds_b200 import lp as L
+    from parallel_ds_b200 import solver as S
+    lp = gen(args.workload, args.solve_one)
+    model = LN.LeavingRowScorer.load(args.weights) if args.pricing == "learned" else None
+    out = []
+    for rep in range(args.repeat):
+        s = S.CudaDualSimplex(S.problem_from_lp(lp), pricing=args.pricing, model=model)
+        s.initDualSimplex()
+        sol = s.solve()
+        out.append(dict(status=s.status(), objective=sol.Z, **{k: v for k, v in s.stats().items()}))
+    print(json.dumps({"workload": args.workload, "seed": args.solve_one, "pricing": args.pricing, "solves": out}))
+    del np
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="learned", choices=sorted(WORKLOADS))
-    ap.add_argument("--pricing", default="dse", choices=["dse", "learned"])
+    ap.add_argument("--pricing", default="learned", choices=["dse", "learned"])
+    ap.add_argument("--weights", default=os.path.join(ROOT, "parallel_ds_b200", "weights",
+                                                      "scorer_m2000_n4000_d1.npz"))
+    ap.add_argument("--tto-lps", type=int, default=4, help="LPs timed alone, learned and plain")
     ap.add_argument("--concurrency", type=int, default=8, help="LPs solved at once per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--solve-one", type=int, default=None, metavar="SEED",
+                    help="solve one LP of the workload alone and print its stats (profiling)")
+    ap.add_argument("--repeat", type=int, default=1, help="--solve-one: solves of the same LP")
     args = ap.parse_args()
+    if args.solve_one is not None:
+        solve_one(args)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

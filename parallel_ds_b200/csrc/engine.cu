@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -41,21 +42,48 @@ constexpr double PERTURB_RATIO = 0.25;
 constexpr double PSI = 1e-5;
 constexpr double EPS_COSTS = 1e-8;
 constexpr double INF_OBJ = 1e25;
-constexpr int BATCH_ITERS = 32;
+// Iteration graphs enqueued per host synchronisation.  A batch never crosses
+// the refactor boundary; an event raised earlier in the batch halts the
+// iteration and the batch's remaining launches return at once (a few
+// microseconds each), so long batches cost little and save host round trips.
+constexpr int BATCH_ITERS = 100;
+
+// Blocks freed to the device's default memory pool stay cached for reuse
+// (release threshold: unlimited) instead of going back to the driver at each
+// synchronisation.  Once per device, per process.
+static void keep_pool_memory(int dev) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), dev) != done.end()) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    done.push_back(dev);
+}
 
 template <typename T>
 struct DBuf {
+    // Stream-ordered device buffer.  A reallocation frees the old block in the
+    // owning stream's order (work already queued there that reads it finishes
+    // first) without the device-wide synchronisation of cudaFree, so solver
+    // handles growing their buffers do not stall one another; growth is
+    // geometric, so a solve whose factor grows reallocates a few times only.
     T* p = nullptr;
     size_t n = 0;
-    void alloc(size_t count) {
-        free();
+    cudaStream_t s = nullptr;
+    void alloc(cudaStream_t st, size_t count) {
+        release();
         if (count == 0) count = 1;
-        CK(cudaMalloc(&p, count * sizeof(T)));
+        CK(cudaMallocAsync(&p, count * sizeof(T), st));
         n = count;
+        s = st;
     }
-    void ensure(size_t count) { if (count > n) alloc(count); }
-    void free() { if (p) cudaFree(p); p = nullptr; n = 0; }
-    ~DBuf() { free(); }
+    void ensure(cudaStream_t st, size_t count) { if (count > n) alloc(st, std::max(count, n + n / 2)); }
+    void release() { if (p) cudaFreeAsync(p, s); p = nullptr; n = 0; }
+    ~DBuf() { if (p) cudaFree(p); }      // handle teardown: its stream may already be gone
 };
 
 struct Engine {
@@ -107,7 +135,6 @@ struct Engine {
     cudaGraphExec_t gexec = nullptr;
     int cap = 0;
     int k = 0;
-    size_t k_alloc = 0;
 
     // solver state kept on the host
     int status = DS_STATUS_UNSOLVED;
@@ -141,6 +168,7 @@ struct Engine {
         if (opt.stream) stream = (cudaStream_t)opt.stream;
         else { CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking)); own_stream = true; }
         CK(cudaMallocHost(&hc, sizeof(Ctl)));
+        keep_pool_memory(opt.device);
         CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
         CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
         CK(cudaEventCreate(&evr0)); CK(cudaEventCreate(&evr1));
@@ -161,7 +189,7 @@ struct Engine {
 
     template <typename T>
     void up(DBuf<T>& b, const std::vector<T>& v) {
-        b.ensure(v.size());
+        b.ensure(stream, v.size());
         if (!v.empty()) CK(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, stream));
     }
 
@@ -208,26 +236,26 @@ struct Engine {
         up(d_cptr, h_cptr); up(d_crow, h_crow); up(d_cval, h_cval);
         up(d_lb, h_lb); up(d_ub, h_ub); up(d_cost, h_cost); up(d_type, h_type);
         // iteration state
-        d_x.ensure(N); d_d.ensure(N); d_beta.ensure(m); d_f.ensure(m);
-        d_basis.ensure(m); d_nonbasis.ensure(n); d_var_pos.ensure(N); d_blocked.ensure(N);
-        d_s_pos.ensure(m); d_s_var.ensure(m); d_rp_row.ensure(m); d_pos_kidx.ensure(m);
-        d_row_slackpos.ensure(m); d_row_kidx.ensure(m);
-        d_cpl_ptr.ensure(m + 1); d_cpl_col.ensure(std::max(nnz, 1)); d_cpl_val.ensure(std::max(nnz, 1));
+        d_x.ensure(stream, N); d_d.ensure(stream, N); d_beta.ensure(stream, m); d_f.ensure(stream, m);
+        d_basis.ensure(stream, m); d_nonbasis.ensure(stream, n); d_var_pos.ensure(stream, N); d_blocked.ensure(stream, N);
+        d_s_pos.ensure(stream, m); d_s_var.ensure(stream, m); d_rp_row.ensure(stream, m); d_pos_kidx.ensure(stream, m);
+        d_row_slackpos.ensure(stream, m); d_row_kidx.ensure(stream, m);
+        d_cpl_ptr.ensure(stream, m + 1); d_cpl_col.ensure(stream, std::max(nnz, 1)); d_cpl_val.ensure(stream, std::max(nnz, 1));
         cap = std::min(std::max(opt.refactor_interval, 1), 200) + 5;
         CK(init_kernel_attributes(cap));
-        d_eta.ensure((size_t)cap * m); d_Mtri.ensure((size_t)cap * cap); d_eta_pos.ensure(cap); d_ybt_pos.ensure(cap + 1);
-        d_rho.ensure(m); d_alpha.ensure(n); d_theta.ensure(n); d_cand.ensure(n); d_ybt.ensure(m);
-        d_btr_rhs.ensure(m); d_aq.ensure(m); d_cc.ensure(m); d_alpha_q.ensure(m); d_tau.ensure(m); d_dxb.ensure(m);
-        for (auto& b : d_y0) b.ensure(m);
-        d_seta.ensure((size_t)MAX_FTRAN_RHS * cap);
+        d_eta.ensure(stream, (size_t)cap * m); d_Mtri.ensure(stream, (size_t)cap * cap); d_eta_pos.ensure(stream, cap); d_ybt_pos.ensure(stream, cap + 1);
+        d_rho.ensure(stream, m); d_alpha.ensure(stream, n); d_theta.ensure(stream, n); d_cand.ensure(stream, n); d_ybt.ensure(stream, m);
+        d_btr_rhs.ensure(stream, m); d_aq.ensure(stream, m); d_cc.ensure(stream, m); d_alpha_q.ensure(stream, m); d_tau.ensure(stream, m); d_dxb.ensure(stream, m);
+        for (auto& b : d_y0) b.ensure(stream, m);
+        d_seta.ensure(stream, (size_t)MAX_FTRAN_RHS * cap);
         const int nb = std::max((m + 255) / 256, (n + 255) / 256) + 8;
-        d_red.ensure(2 * nb); d_redi.ensure(4 * nb);
-        d_flip.ensure(n); d_flip_list.ensure(n);
-        d_tmp_rows.ensure(m); d_tmp_rows2.ensure(m); d_tmp_pos.ensure(m); d_tmp_pos2.ensure(m); d_h.ensure(cap);
-        d_ctl.ensure(1);
-        d_Winv.ensure(16 * 16); d_ferr.ensure(1);
-        d_trace.ensure(2); d_trace_d.ensure(2);
-        d_score.ensure(m); d_enter_cnt.ensure(N); d_entered_at.ensure(N);
+        d_red.ensure(stream, 2 * nb); d_redi.ensure(stream, 4 * nb);
+        d_flip.ensure(stream, n); d_flip_list.ensure(stream, n);
+        d_tmp_rows.ensure(stream, m); d_tmp_rows2.ensure(stream, m); d_tmp_pos.ensure(stream, m); d_tmp_pos2.ensure(stream, m); d_h.ensure(stream, cap);
+        d_ctl.ensure(stream, 1);
+        d_Winv.ensure(stream, 16 * 16); d_ferr.ensure(stream, 1);
+        d_trace.ensure(stream, 2); d_trace_d.ensure(stream, 2);
+        d_score.ensure(stream, m); d_enter_cnt.ensure(stream, N); d_entered_at.ensure(stream, N);
         std::vector<int> rc(m);
         for (int i = 0; i < m; ++i) rc[i] = h_rptr[i + 1] - h_rptr[i];
         up(d_row_nnz, rc);
@@ -266,8 +294,8 @@ struct Engine {
         }
         up(d_pd_c, c); up(d_pd_lo, lo); up(d_pd_hi, hi); up(d_pd_L, L); up(d_pd_U, U);
         up(d_pd_tau, tau); up(d_pd_sigma, sig);
-        d_pd_x.ensure(n); d_pd_xbar.ensure(n); d_pd_xsum.ensure(n); d_pd_y.ensure(m); d_pd_ysum.ensure(m);
-        d_pd_gap.ensure(N); d_pd_dual.ensure(N);
+        d_pd_x.ensure(stream, n); d_pd_xbar.ensure(stream, n); d_pd_xsum.ensure(stream, n); d_pd_y.ensure(stream, m); d_pd_ysum.ensure(stream, m);
+        d_pd_gap.ensure(stream, N); d_pd_dual.ensure(stream, N);
         if (pd_gexec) { cudaGraphExecDestroy(pd_gexec); pd_gexec = nullptr; }
     }
 
@@ -389,11 +417,9 @@ struct Engine {
         put(d_cpl_ptr, cptr); put(d_cpl_col, ccol);
         if (!cval.empty()) CK(cudaMemcpyAsync(d_cpl_val.p, cval.data(), cval.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
         const size_t kk = (size_t)std::max(k, 1) * std::max(k, 1);
-        if (kk > k_alloc) {
-            d_Kinv.alloc(kk); d_S.alloc(kk); k_alloc = kk;
-        }
-        d_Pan.ensure((size_t)std::max(k, 1) * 16); d_Wk.ensure((size_t)std::max(k, 1) * 16);
-        d_rowpiv.ensure(std::max(k, 1)); d_piv_rows.ensure(std::max(k, 1));
+        d_Kinv.ensure(stream, kk); d_S.ensure(stream, kk);
+        d_Pan.ensure(stream, (size_t)std::max(k, 1) * 16); d_Wk.ensure(stream, (size_t)std::max(k, 1) * 16);
+        d_rowpiv.ensure(stream, std::max(k, 1)); d_piv_rows.ensure(stream, std::max(k, 1));
         // FTRAN launch geometry for this k
         const int tile = 256;
         const int ntile = std::max(1, (k + tile - 1) / tile);
@@ -402,8 +428,8 @@ struct Engine {
         int chunk = std::max(16, (k + want - 1) / want);
         const int nchunk = std::max(1, (k + chunk - 1) / chunk);
         D.ftr_tile = tile; D.ftr_chunk = chunk; D.ftr_ntile = ntile; D.ftr_nchunk = nchunk;
-        d_part.ensure((size_t)nchunk * MAX_FTRAN_RHS * std::max(k, 1));
-        d_tile_tickets.ensure(ntile);
+        d_part.ensure(stream, (size_t)nchunk * MAX_FTRAN_RHS * std::max(k, 1));
+        d_tile_tickets.ensure(stream, ntile);
         CK(cudaMemsetAsync(d_tile_tickets.p, 0, sizeof(unsigned) * ntile, stream));
         sync_dev();
         FactorBufs F{d_S.p, d_Pan.p, d_Wk.p, d_rowpiv.p, d_piv_rows.p, d_Winv.p, d_ferr.p, d_s_var.p, d_row_kidx.p};
@@ -939,7 +965,7 @@ struct Engine {
         CK(cudaMemcpyAsync(d_var_pos.p, vp.data(), sizeof(int) * N, cudaMemcpyHostToDevice, stream));
         refactor();
         DBuf<double> in, o;
-        in.alloc((size_t)nr * m); o.alloc((size_t)nr * m);
+        in.alloc(stream, (size_t)nr * m); o.alloc(stream, (size_t)nr * m);
         CK(cudaMemcpyAsync(in.p, rhs, sizeof(double) * nr * m, cudaMemcpyHostToDevice, stream));
         for (int r0 = 0; r0 < nr; r0 += (transpose ? 1 : MAX_FTRAN_RHS)) {
             if (transpose) {
@@ -1003,14 +1029,14 @@ struct Engine {
         CK(cudaMemsetAsync(d_aq.p, 0, sizeof(double) * m, stream));
         CK(cudaMemsetAsync(d_enter_cnt.p, 0, sizeof(int) * N, stream));
         CK(cudaMemsetAsync(d_entered_at.p, 0, sizeof(int) * N, stream));
-        d_trace.alloc(2 * std::max(trace_cap, 1)); d_trace_d.alloc(2 * std::max(trace_cap, 1));
+        d_trace.alloc(stream, 2 * std::max(trace_cap, 1)); d_trace_d.alloc(stream, 2 * std::max(trace_cap, 1));
         if (opt.pricing == DS_PRICING_LEARNED && !mlp)
             throw CudaError("learned pricing needs a model (ds_set_model)", DS_ERR_STATE);
         if (mlp && model_device(mlp) != opt.device)
             throw CudaError("model lives on another device", DS_ERR_STATE);
         if (ftr_every > 0) {
-            d_ftr_feat.ensure((size_t)ftr_cap * DS_NUM_FEATURES);
-            d_ftr_meta.ensure((size_t)ftr_cap * 3);
+            d_ftr_feat.ensure(stream, (size_t)ftr_cap * DS_NUM_FEATURES);
+            d_ftr_meta.ensure(stream, (size_t)ftr_cap * 3);
         }
         invalidate_graph();   // launch parameters may have changed
         const bool want_pd = (opt.pricing == DS_PRICING_LEARNED) || ftr_every > 0;
