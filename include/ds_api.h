@@ -272,6 +272,58 @@ int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, const double
 int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos,
                         const double* rhs, double* sol, int transpose);
 
+/* ---- batched persistent solver -------------------------------------------------
+ * No counterpart in the reference.  Many independent LPs
+ *     min c^T x  s.t.  A x <= b,  x >= 0        (m <= DS_BATCH_MAX_M, any n)
+ * solved in one persistent launch (CUDA graph), each by the reference's dual
+ * simplex rules (DSE pricing, textbook ratio test with the EPS_Z tie rule)
+ * on a dense explicit basis inverse.  The slack basis must be dual feasible
+ * (c >= 0); other instances get DS_STATUS_ERROR and belong on ds_solve, which
+ * has phase 1.  Statuses: DS_STATUS_OPTIMAL, DS_STATUS_PRIMAL_INFEASIBLE,
+ * DS_STATUS_ITER_LIMIT (50 m iterations, at least 1000), DS_STATUS_ERROR. */
+#define DS_BATCH_MAX_M 1024
+typedef struct ds_batch ds_batch;
+typedef struct ds_batch_stats {
+    int       count;            /* instances loaded                                */
+    int       buckets;          /* m-buckets of the schedule                       */
+    int       block;            /* threads per CTA of the persistent launch        */
+    double    solve_ms;         /* device time of the last ds_batch_solve          */
+    double    tune_ms;          /* device time of the last ds_batch_tune           */
+    long long total_nnz;
+    char      schedule[512];    /* group size and B^-1 placement per bucket        */
+} ds_batch_stats;
+int ds_batch_create(int device, ds_batch** out);
+int ds_batch_destroy(ds_batch* b);
+const char* ds_batch_last_error(const ds_batch* b);
+/* count instances, concatenated: instance i has m[i] rows, n[i] columns, column
+ * pointers col_ptr (n[i]+1 entries starting at 0), row_idx/val (col_ptr[n[i]]
+ * entries), rhs (m[i]) and cost (n[i]).  Inputs are copied.  m[i] above
+ * DS_BATCH_MAX_M returns DS_ERR_CAPACITY.  Reloading instances of the same
+ * shapes keeps the schedule (tuned or set) and the captured launch. */
+int ds_batch_load(ds_batch* b, int count, const int* m, const int* n, const int* col_ptr, const int* row_idx,
+                  const double* val, const double* rhs, const double* cost);
+/* Generate and load count instances of the seeded generator (instance i: seed
+ * + i, m ~ U{m_lo..m_hi} by ds_gen_batch_m, n = 2m, Bernoulli(density)). */
+int ds_batch_generate(ds_batch* b, int count, int m_lo, int m_hi, double density, unsigned long long seed);
+/* The same instances into caller arrays (the ds_batch_load layout).  Call with
+ * col_ptr == NULL first: sizes[0..3] receive the lengths of col_ptr, row_idx /
+ * val, rhs and cost, and m/n (count each, may be NULL) the shapes. */
+long long ds_batch_gen_arrays(int count, int m_lo, int m_hi, double density, unsigned long long seed, int* m,
+                              int* n, int* col_ptr, int* row_idx, double* val, double* rhs, double* cost,
+                              long long* sizes);
+/* Autotune the schedule: per m-bucket group size (32..512 threads) and B^-1
+ * placement (shared or global memory), and the CTA size, timed on samples. */
+int ds_batch_tune(ds_batch* b);
+/* Set the schedule by hand: block in {128, 256, 512}; per bucket (largest m
+ * first) the group size and whether B^-1 sits in shared memory. */
+int ds_batch_set_schedule(ds_batch* b, int block, const int* group_size, const int* binv_in_smem, int nbuckets);
+int ds_batch_num_buckets(const ds_batch* b);
+int ds_batch_solve(ds_batch* b);
+int ds_batch_get_results(const ds_batch* b, int* status, double* objective, int* iterations);
+/* Instance i: x (n[i] structurals) and row duals y (m[i]); either may be NULL. */
+int ds_batch_get_solution(const ds_batch* b, int i, double* x, double* y);
+int ds_batch_get_stats(const ds_batch* b, ds_batch_stats* st);
+
 /* ---- seeded LP generator (shared by tests, bench and the trainer) ---------- */
 #define DS_GEN_DENSITY   0   /* Bernoulli(density) per entry                   */
 #define DS_GEN_PER_COL   1   /* exactly per_col nonzeros per column            */
