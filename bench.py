@@ -331,7 +331,8 @@ def batch_arm(args, rank, world, local_rank):
     arr = gen_arrays(count, cfg["m_lo"], cfg["m_hi"], cfg["density"], seed, alloc=pinned)
     bs = BatchSolver(local_rank)
     bs.load_arrays(arr)
-    bs.tune()                                   # untimed: the autotuner picks the schedule
+    if not args.no_tune:
+        bs.tune()                               # untimed: the autotuner picks the schedule
     for _ in range(args.warmup):
         bs.solve()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
@@ -416,25 +417,27 @@ def batch_arm(args, rank, world, local_rank):
     }
 
 
-def batch_cpu_sample(workload, seconds=15.0, threads=1):
-    """The oracle solving the batch's first instances one after another on
-    `threads` host threads until about `seconds` have passed."""
+def batch_cpu_sample(workload, seconds=15.0, threads=1, max_lps=4096):
+    """The oracle solving the batch's first instances (generated before the
+    clock starts) on `threads` host threads until about `seconds` have passed."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import pyoracle as po
     from parallel_ds_b200 import lp as L
     cfg = BATCH[workload]
+    lps = [L.typed(L.batched_instance(cfg["seed"], i, cfg["m_lo"], cfg["m_hi"], cfg["density"]))
+           for i in range(min(max_lps, cfg["count"]))]
     t0 = time.perf_counter()
     done, statuses = 0, set()
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        while time.perf_counter() - t0 < seconds and done < cfg["count"]:
-            lps = [L.typed(L.batched_instance(cfg["seed"], done + k, cfg["m_lo"], cfg["m_hi"], cfg["density"]))
-                   for k in range(min(threads, cfg["count"] - done))]
-            for r in ex.map(po.solve_typed, lps):
+        while time.perf_counter() - t0 < seconds and done < len(lps):
+            chunk = lps[done:done + 4 * threads]
+            for r in ex.map(po.solve_typed, chunk):
                 statuses.add(r["status"])
-            done += len(lps)
+            done += len(chunk)
     dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": "LPs/s", "cores": threads, "kind": "port",
-            "sample": f"oracle solves the batch's first {done} instances ({sorted(statuses)}), {dt:.1f} s"}
+            "sample": f"oracle solves the batch's first {done} instances ({sorted(statuses)}) on {threads} "
+                      f"thread(s), {dt:.1f} s"}
 
 
 def _status(code):
@@ -521,7 +524,8 @@ def solve_one(args):
     model = LN.LeavingRowScorer.load(args.weights) if args.pricing == "learned" else None
     out = []
     for rep in range(args.repeat):
-        s = S.CudaDualSimplex(S.problem_from_lp(lp), pricing=args.pricing, model=model)
+        kw = {"max_iterations": args.max_iterations} if args.max_iterations else {}
+        s = S.CudaDualSimplex(S.problem_from_lp(lp), pricing=args.pricing, model=model, **kw)
         s.initDualSimplex()
         sol = s.solve()
         out.append(dict(status=s.status(), objective=sol.Z, **{k: v for k, v in s.stats().items()}))
@@ -545,6 +549,8 @@ def main():
     ap.add_argument("--solve-one", type=int, default=None, metavar="SEED",
                     help="solve one LP of the workload alone and print its stats (profiling)")
     ap.add_argument("--repeat", type=int, default=1, help="--solve-one: solves of the same LP")
+    ap.add_argument("--no-tune", action="store_true", help="batched workloads: default schedule, no autotuning")
+    ap.add_argument("--max-iterations", type=int, default=0, help="--solve-one: iteration cap (0: none)")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="batched workloads: LPs per GPU (default: the workload's 4096 / 65,536)")
     args = ap.parse_args()
