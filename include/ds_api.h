@@ -77,6 +77,10 @@ typedef struct ds_options {
                                   iterations of the warm-start estimate whose
                                   bound gaps and duals are network features
                                   (default 4000; 0 = off)                         */
+    int    dense_max_m;        /* m <= this: keep B^-1 explicitly (m*m doubles) and
+                                  update it by a rank-1 step per iteration instead of
+                                  the eta file; exact DSE weights (default 4096;
+                                  0 = always the eta file)                        */
 } ds_options;
 
 typedef struct ds_stats {

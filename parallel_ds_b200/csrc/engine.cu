@@ -124,6 +124,11 @@ struct Engine {
     DBuf<double> d_pd_c, d_pd_lo, d_pd_hi, d_pd_L, d_pd_U, d_pd_tau, d_pd_sigma;
     DBuf<double> d_pd_x, d_pd_xbar, d_pd_xsum, d_pd_y, d_pd_ysum;
     DBuf<float> d_pd_gap, d_pd_dual;
+    // dense mode: explicit B^-1
+    bool dense = false;
+    DBuf<double> d_Binv, d_binv_part;
+    DBuf<unsigned> d_binv_tickets;
+    static constexpr int BINV_RC = 32;    // rows of B^-1 per chunk of the tiled kernels
     PdhgDev PD{};
     cudaGraphExec_t pd_gexec = nullptr;
     static constexpr int PDHG_RESTART = 500;
@@ -256,6 +261,14 @@ struct Engine {
         d_Winv.ensure(stream, 16 * 16); d_ferr.ensure(stream, 1);
         d_trace.ensure(stream, 2); d_trace_d.ensure(stream, 2);
         d_score.ensure(stream, m); d_enter_cnt.ensure(stream, N); d_entered_at.ensure(stream, N);
+        dense = opt.dense_max_m > 0 && m <= opt.dense_max_m;
+        if (dense) {
+            const int chunks = (m + BINV_RC - 1) / BINV_RC;
+            d_Binv.ensure(stream, (size_t)m * m);
+            d_binv_part.ensure(stream, (size_t)chunks * m);
+            d_binv_tickets.ensure(stream, (size_t)(m + 255) / 256 + 1);
+            CK(cudaMemsetAsync(d_binv_tickets.p, 0, sizeof(unsigned) * ((m + 255) / 256 + 1), stream));
+        }
         std::vector<int> rc(m);
         for (int i = 0; i < m; ++i) rc[i] = h_rptr[i + 1] - h_rptr[i];
         up(d_row_nnz, rc);
@@ -362,6 +375,9 @@ struct Engine {
         D.ftr_every = ftr_every; D.ftr_cap = ftr_cap;
         D.ftr_feat = d_ftr_feat.p; D.ftr_meta = d_ftr_meta.p;
         D.pd_gap = d_pd_gap.p; D.pd_dual = d_pd_dual.p;
+        D.dense = dense ? 1 : 0;
+        D.Binv = d_Binv.p; D.binv_part = d_binv_part.p; D.binv_tickets = d_binv_tickets.p;
+        D.binv_rc = BINV_RC; D.binv_chunks = (m + BINV_RC - 1) / BINV_RC;
         D.ctl = d_ctl.p;
         D.tile_tickets = d_tile_tickets.p;
     }
@@ -473,6 +489,7 @@ struct Engine {
                 }
             fprintf(stderr, "[ds-check] refactor it %d k %d |Kinv K - I| %.3e (%.2f ms)\n", hc->iteration, k, worst, ms);
         }
+        if (dense) CK(launch_binv_build(D, stream));   // B^-1 of the new B0 (D.k set by sync_dev above)
         hc->T = 0;
         hc->k = k;
         push();
@@ -504,17 +521,24 @@ struct Engine {
     // -------------------------------------------------------------- solves
     // FTRAN of one dense row vector: out = B^-1 rhs (solveLinSys, transpose=false)
     void ftran1(const double* rhs, double* out) {
+        if (dense) { CK(launch_dense_ftran_vec(D, rhs, out, stream)); return; }
         Dev E = D;
         E.frhs[0] = rhs; E.fout[0] = out;
         CK(launch_ftran(E, 1, 0, 1, stream));
     }
     void ftran2(const double* r0, double* o0, const double* r1, double* o1) {
+        if (dense) {
+            CK(launch_dense_ftran_vec(D, r0, o0, stream));
+            CK(launch_dense_ftran_vec(D, r1, o1, stream));
+            return;
+        }
         Dev E = D;
         E.frhs[0] = r0; E.fout[0] = o0; E.frhs[1] = r1; E.fout[1] = o1;
         CK(launch_ftran(E, 2, 0, 1, stream));
     }
     // BTRAN of a dense position vector: y = B^-T c (rows)
     void btran_dense(const double* c0, double* y) {
+        if (dense) { CK(launch_dense_btran_vec(D, c0, y, stream)); return; }
         CK(launch_btran_dense_eta(D, c0, d_h.p, hc->T, stream));
         CK(launch_btran_b0(D, y, 1, stream));
     }
@@ -540,6 +564,11 @@ struct Engine {
         if (ibasis) {
             std::vector<double> ones(m, 1.0);
             CK(cudaMemcpyAsync(d_beta.p, ones.data(), sizeof(double) * m, cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+            return;
+        }
+        if (dense) {                 // exact weights from the explicit inverse
+            CK(launch_dense_beta(D, stream));
             CK(cudaStreamSynchronize(stream));
             return;
         }
@@ -677,6 +706,16 @@ struct Engine {
         pull();
         clear_event(); push();
         const int nr = hc->nrhs;
+        if (dense) {
+            // rebuild B^-1 for the current basis, then redo rho, the FTRAN and the
+            // update of this iteration with it
+            refactor();
+            CK(launch_dense_rho(D, hc->p_idx, stream));
+            CK(launch_ftran_dense(D, 0, 1, stream));
+            CK(launch_update_forced(D, stream));
+            CK(launch_binv_update(D, 1, stream));
+            return;
+        }
         refactor();
         if (nr > 2) ftran2(d_rho.p, d_tau.p, d_cc.p, d_dxb.p);
         else ftran1(d_rho.p, d_tau.p);
@@ -699,7 +738,9 @@ struct Engine {
             case S_FTRAN_K: return 8 * K * K + 16 * R * K + 8 * R * K * D.ftr_nchunk;
             case S_FTRAN_ASM: return 20.0 * nnz_cpl + (M - K) * (4 + 16 * R) + 8 * R * Tt;
             case S_ETA_APPLY: return 8 * Tt * M + 16 * R * M;
-            case S_UPDATE: return 60 * M + 8 * Tt + 4 * Tt * Tt;
+            case S_UPDATE: return dense ? 44 * M : 60 * M + 8 * Tt + 4 * Tt * Tt;
+            case S_FTRAN_DENSE: return (12.0 + 8 * M) * ((double)h_rptr[m] / n) + 8 * M;
+            case S_BINV: return 16 * M * M + 16 * M + 8 * M * ((M + BINV_RC - 1) / BINV_RC);
         }
         return 0;
     }
@@ -799,8 +840,7 @@ struct Engine {
             const int T0 = hc->T;
             bool ran[S_NSTEPS] = {};
             for (int stp = 0; stp < S_NSTEPS; ++stp) {
-                if ((stp == S_BTRAN_RHS || stp == S_FTRAN_K) && k == 0) continue;
-                if (stp == S_SCORE && !score_step_active(D)) continue;
+                if (!step_active(D, stp)) continue;
                 CK(cudaEventRecord(pev[2 * stp], stream));
                 CK(launch_step(D, stp, stream));
                 CK(cudaEventRecord(pev[2 * stp + 1], stream));
@@ -1157,6 +1197,7 @@ void ds_default_options(ds_options* o) {
     o->verbose = 0;
     o->learned_mix = 0.05;
     o->learned_pdhg_iters = 4000;
+    o->dense_max_m = 4096;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }

@@ -145,6 +145,13 @@ struct Dev {
     int* ftr_meta;              // ftr_cap x 3: iteration, position, variable
     const float* pd_gap;        // N: PDHG estimate's distance to the nearest bound
     const float* pd_dual;       // N: PDHG estimate's dual magnitude
+    // dense mode (m <= ds_options.dense_max_m): explicit B^-1, column r (constraint
+    // row r) contiguous over basis positions: Binv[r * m + i] = (B^-1)_{i r}
+    int dense;
+    double* Binv;               // m * m
+    double* binv_part;          // binv_chunks * m partial sums (exact DSE weights, dense FTRAN)
+    unsigned* binv_tickets;     // one per column tile of BS positions
+    int binv_rc, binv_chunks;   // rows of B^-1 per chunk, chunk count
     Ctl* ctl;
     // launch geometry (set per factor)
     int ftr_tile, ftr_chunk, ftr_ntile, ftr_nchunk;

@@ -449,7 +449,14 @@ __global__ void k_chuzr(Dev D) {
         }
     }
     __syncthreads();
-    if (s_pidx >= 0) btran_unit_eta<BS>(D, s_pidx, Gs);
+    if (s_pidx >= 0) {
+        if (D.dense) {
+            // rho = B^-T e_p = row p of the explicit inverse
+            for (int r = threadIdx.x; r < D.m; r += BS) D.rho[r] = D.Binv[(size_t)r * D.m + s_pidx];
+        } else {
+            btran_unit_eta<BS>(D, s_pidx, Gs);
+        }
+    }
 }
 
 // Standalone eta part of BTRAN for e_{p_idx} (exact DSE weight recomputation).
@@ -1001,10 +1008,12 @@ __global__ void k_update(Dev D, int force) {
         } else if (i != p_idx) {
             D.f[i] = D.f[i] - aqi * theta_P;
         }
-        D.eta[(size_t)T * D.m + i] = (i != p_idx) ? -aqi / ap : 1 / ap;
-        if (i != p_idx) {
-            const double r = aqi / ap;
-            D.beta[i] = D.beta[i] - 2 * aqi / ap * D.tau[i] + (r * r) * bp;
+        if (!D.dense) {   // dense mode: B^-1 and exact DSE weights are updated by k_binv_update
+            D.eta[(size_t)T * D.m + i] = (i != p_idx) ? -aqi / ap : 1 / ap;
+            if (i != p_idx) {
+                const double r = aqi / ap;
+                D.beta[i] = D.beta[i] - 2 * aqi / ap * D.tau[i] + (r * r) * bp;
+            }
         }
     }
     if (phase == 2 && nflips > 0) {
@@ -1015,7 +1024,7 @@ __global__ void k_update(Dev D, int force) {
     __shared__ double g[1024];
     if (threadIdx.x == 0) {
         const int p = c->p, q = c->q, q_idx = c->q_idx;
-        D.beta[p_idx] = bp / (ap * ap);
+        if (!D.dense) D.beta[p_idx] = bp / (ap * ap);
         if (phase == 2) {
             double dz = c->dz;
             if (nflips > 0) for (int b = 0; b < (int)gridDim.x; ++b) dz -= __ldcg(&D.red[b]);
@@ -1044,7 +1053,7 @@ __global__ void k_update(Dev D, int force) {
         } else {
             c->cycle = (fabs(theta) < EPS_A) ? c->cycle + 1 : 0;
         }
-        D.eta_pos[T] = p_idx;
+        if (!D.dense) D.eta_pos[T] = p_idx;
         c->pivots += 1;
         if (phase == 2 && c->trace_n < c->trace_cap) {
             const int tn = c->trace_n;
@@ -1053,6 +1062,7 @@ __global__ void k_update(Dev D, int force) {
         }
         if (phase == 2) c->trace_n += 1;
     }
+    if (D.dense) return;   // no eta file in dense mode
     // new row of G: G[T][u] = eta_u[p_T] - [p_u == p_T]
     for (int u = threadIdx.x; u < T; u += BS)
         g[u] = D.eta[(size_t)u * D.m + p_idx] - (D.eta_pos[u] == p_idx ? 1.0 : 0.0);
@@ -1314,7 +1324,17 @@ cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaS
 // One kernel of the iteration sequence (profiling launches them one by one).
 const char* const kStepNames[S_NSTEPS] = {"k_mlp_score", "k_chuzr", "k_btran_rhs", "k_btran_gemv", "k_pivot_row",
                                           "k_dual_update", "k_ftran_k", "k_ftran_assemble", "k_eta_apply",
-                                          "k_update"};
+                                          "k_ftran_dense", "k_update", "k_binv_update"};
+
+bool step_active(const Dev& D, int step) {
+    switch (step) {
+        case S_SCORE: return score_step_active(D);
+        case S_BTRAN_RHS: case S_FTRAN_K: return !D.dense && D.k > 0;
+        case S_BTRAN_GEMV: case S_FTRAN_ASM: case S_ETA_APPLY: return !D.dense;
+        case S_FTRAN_DENSE: case S_BINV: return D.dense != 0;
+        default: return true;
+    }
+}
 
 
 static cudaError_t set_kernel_attributes(int cap);
@@ -1341,7 +1361,10 @@ static cudaError_t set_kernel_attributes(int cap) {
 }
 
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
+    if (step != S_SCORE && !step_active(D, step)) return cudaSuccess;
     switch (step) {
+        case S_FTRAN_DENSE: return launch_ftran_dense(D, 1, 0, s);
+        case S_BINV: return launch_binv_update(D, 0, s);
         case S_SCORE: return launch_score(D, s);
         case S_CHUZR: k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D); break;
         case S_BTRAN_RHS: if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, 0); else return cudaSuccess; break;
@@ -1489,6 +1512,218 @@ cudaError_t launch_pivot_row_mode(const Dev& D, int mode, cudaStream_t s) {
 
 cudaError_t launch_phase1_init(const Dev& D, double* cc, cudaStream_t s) {
     k_phase1_init<BS><<<1, BS, 0, s>>>(D, cc);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+// ================================================================ dense mode
+// The explicit inverse replaces the eta file for m up to ds_options.dense_max_m:
+// Binv[r * m + i] = (B^-1)_{i r} (constraint row r, basis position i), so an
+// FTRAN gathers whole columns (coalesced over positions) and the rank-1 update
+// streams B^-1 once per iteration across every SM.
+
+// B^-1 from the factor of B0 = P [K 0; C I]:  for a K row kr (constraint row
+// r = rp_row[kr]) column r holds Kinv[:, kr] at the structural positions and
+// -C Kinv[:, kr] at the slack positions; a slack row's column is a unit vector.
+template <int BS>
+__global__ void k_binv_struct(Dev D) {
+    const int kr = blockIdx.x, k = D.k;
+    const size_t r = (size_t)D.rp_row[kr];
+    for (int c = threadIdx.x; c < k; c += BS) D.Binv[r * D.m + D.s_pos[c]] = D.Kinv[(size_t)kr * k + c];
+}
+template <int BS>
+__global__ void k_binv_coupling(Dev D) {
+    const int kr = blockIdx.x, k = D.k;
+    const int rr = blockIdx.y * BS + threadIdx.x;
+    if (rr >= D.m) return;
+    const int sp = D.row_slackpos[rr];
+    if (sp < 0) return;
+    const double* kc = D.Kinv + (size_t)kr * k;
+    double s = 0.0;
+    for (int e = D.cpl_ptr[rr]; e < D.cpl_ptr[rr + 1]; ++e) s += D.cpl_val[e] * kc[D.cpl_col[e]];
+    D.Binv[(size_t)D.rp_row[kr] * D.m + sp] = -s;
+}
+__global__ void k_binv_unit(Dev D) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= D.m) return;
+    const int sp = D.row_slackpos[r];
+    if (sp >= 0) D.Binv[(size_t)r * D.m + sp] = 1.0;
+}
+
+__global__ void k_dense_rho(Dev D, int p_idx) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < D.m) D.rho[r] = D.Binv[(size_t)r * D.m + p_idx];
+}
+
+// Iteration FTRAN: alpha_q = B^-1 a_q (a_q: CSC column or unit slack column) and,
+// with bound flips, dx_B = B^-1 column_change; then the pivot check of k_eta_apply.
+template <int BS>
+__global__ void k_ftran_dense(Dev D, int check, int force) {
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int q = c->q, nr = c->nrhs;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    const size_t M = D.m;
+    if (i < D.m) {
+        double s = 0.0;
+        if (q < D.n) {
+#pragma unroll 4
+            for (int e = D.cptr[q]; e < D.cptr[q + 1]; ++e) s += D.Binv[(size_t)D.crow[e] * M + i] * D.cval[e];
+        } else {
+            s = D.Binv[(size_t)(q - D.n) * M + i];
+        }
+        D.alpha_q[i] = s;
+        if (nr > 2) {
+            double t = 0.0;
+            for (int r = 0; r < D.m; ++r) {
+                const double v = D.cc[r];
+                if (v != 0.0) t += D.Binv[(size_t)r * M + i] * v;
+            }
+            D.dxb[i] = t;
+        }
+    }
+    if (!last_block(&c->tickets[6])) return;
+    if (check && threadIdx.x == 0) {
+        const double aqp = __ldcg(&D.alpha_q[c->p_idx]);
+        const double apq = D.alpha[c->q_idx];
+        if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
+        else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
+    }
+}
+
+// B^-1 <- E B^-1 with E the eta of (alpha_q, p): row p scaled by 1/alpha_p, row i
+// minus alpha_q[i]/alpha_p times row p; fused with the exact DSE weights
+// beta_i = ||row i of B^-1||^2 (chunk partials, summed in chunk order by the
+// last block of each column tile).  Grid: (position tiles, row chunks).
+template <int BS>
+__global__ void k_binv_update(Dev D, int force) {
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int p = c->p_idx;
+    const size_t M = D.m;
+    const double inv = 1.0 / __ldcg(&D.alpha_q[p]);
+    const int i = blockIdx.x * BS + threadIdx.x;
+    const int r0 = blockIdx.y * D.binv_rc, r1 = min(D.m, r0 + D.binv_rc);
+    if (i < D.m) {
+        const double f = D.alpha_q[i];
+        const bool isp = (i == p);
+        double* col = D.Binv + i;
+        double acc = 0.0;
+        int r = r0;
+        for (; r + 8 <= r1; r += 8) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = col[(size_t)(r + u) * M];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const double piv = D.rho[r + u] * inv;
+                const double nv = isp ? piv : v[u] - f * piv;
+                col[(size_t)(r + u) * M] = nv;
+                acc += nv * nv;
+            }
+        }
+        for (; r < r1; ++r) {
+            const double piv = D.rho[r] * inv;
+            const double nv = isp ? piv : col[(size_t)r * M] - f * piv;
+            col[(size_t)r * M] = nv;
+            acc += nv * nv;
+        }
+        D.binv_part[(size_t)blockIdx.y * M + i] = acc;
+    }
+    if (!last_in_tile(&D.binv_tickets[blockIdx.x])) return;
+    if (i < D.m) {
+        double b = 0.0;
+        for (int y = 0; y < (int)gridDim.y; ++y) b += __ldcg(&D.binv_part[(size_t)y * M + i]);
+        D.beta[i] = b;
+    }
+}
+
+// y = B^-1 v (mode 0) or y_i = ||row i of B^-1||^2 (mode 1), same tiling.
+template <int BS>
+__global__ void k_dense_colsum(Dev D, const double* v, double* y, int mode) {
+    const size_t M = D.m;
+    const int i = blockIdx.x * BS + threadIdx.x;
+    const int r0 = blockIdx.y * D.binv_rc, r1 = min(D.m, r0 + D.binv_rc);
+    if (i < D.m) {
+        double acc = 0.0;
+        for (int r = r0; r < r1; ++r) {
+            const double b = D.Binv[(size_t)r * M + i];
+            acc += mode ? b * b : b * v[r];
+        }
+        D.binv_part[(size_t)blockIdx.y * M + i] = acc;
+    }
+    if (!last_in_tile(&D.binv_tickets[blockIdx.x])) return;
+    if (i < D.m) {
+        double s = 0.0;
+        for (int yy = 0; yy < (int)gridDim.y; ++yy) s += __ldcg(&D.binv_part[(size_t)yy * M + i]);
+        y[i] = s;
+    }
+}
+
+// y = B^-T c: one warp per constraint row r, a contiguous dot over positions.
+__global__ void k_dense_btran_vec(Dev D, const double* cpos, double* y) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= D.m) return;
+    const double* col = D.Binv + (size_t)w * D.m;
+    double s = 0.0;
+    for (int i = lane; i < D.m; i += 32) s += col[i] * cpos[i];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) y[w] = s;
+}
+
+cudaError_t launch_binv_build(const Dev& D, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(D.Binv, 0, sizeof(double) * (size_t)D.m * D.m, s);
+    if (e != cudaSuccess) return e;
+    if (D.k > 0) {
+        k_binv_struct<BS><<<D.k, BS, 0, s>>>(D);
+        k_binv_coupling<BS><<<dim3(D.k, nblk(D.m)), BS, 0, s>>>(D);
+        count_launch(2);
+    }
+    k_binv_unit<<<nblk(D.m), BS, 0, s>>>(D);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_dense_rho(const Dev& D, int p_idx, cudaStream_t s) {
+    k_dense_rho<<<nblk(D.m), BS, 0, s>>>(D, p_idx);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_ftran_dense(const Dev& D, int check, int force, cudaStream_t s) {
+    k_ftran_dense<BS><<<nblk(D.m), BS, 0, s>>>(D, check, force);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_binv_update(const Dev& D, int force, cudaStream_t s) {
+    k_binv_update<BS><<<dim3(nblk(D.m), D.binv_chunks), BS, 0, s>>>(D, force);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_dense_ftran_vec(const Dev& D, const double* v, double* y, cudaStream_t s) {
+    k_dense_colsum<BS><<<dim3(nblk(D.m), D.binv_chunks), BS, 0, s>>>(D, v, y, 0);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_dense_btran_vec(const Dev& D, const double* c, double* y, cudaStream_t s) {
+    k_dense_btran_vec<<<(D.m * 32 + BS - 1) / BS, BS, 0, s>>>(D, c, y);
+    count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_dense_beta(const Dev& D, cudaStream_t s) {
+    k_dense_colsum<BS><<<dim3(nblk(D.m), D.binv_chunks), BS, 0, s>>>(D, nullptr, D.beta, 1);
     count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;

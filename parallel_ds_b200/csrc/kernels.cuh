@@ -21,8 +21,11 @@ struct FactorBufs {
 cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s);
 
 // Kernels of one iteration, in launch order.
+// PFI mode runs S_BTRAN_RHS .. S_ETA_APPLY; dense mode runs S_FTRAN_DENSE and S_BINV
+// instead (step_active tells which).
 enum Step : int { S_SCORE = 0, S_CHUZR, S_BTRAN_RHS, S_BTRAN_GEMV, S_PIVOT_ROW, S_DUAL_UPDATE,
-                  S_FTRAN_K, S_FTRAN_ASM, S_ETA_APPLY, S_UPDATE, S_NSTEPS };
+                  S_FTRAN_K, S_FTRAN_ASM, S_ETA_APPLY, S_FTRAN_DENSE, S_UPDATE, S_BINV, S_NSTEPS };
+bool step_active(const Dev& D, int step);
 extern const char* const kStepNames[S_NSTEPS];
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s);
 // S_SCORE: network scores (learned pricing) and/or the feature trace; no
@@ -61,5 +64,14 @@ cudaError_t launch_chuzr_only(const Dev& D, cudaStream_t s);
 // mode bit 1: compute alpha from rho (else alpha is given); bit 2: run CHUZC.
 cudaError_t launch_pivot_row_mode(const Dev& D, int mode, cudaStream_t s);
 cudaError_t launch_build_mtri(const Dev& D, int T, cudaStream_t s);
+
+// Dense mode (explicit B^-1).
+cudaError_t launch_binv_build(const Dev& D, cudaStream_t s);             // after factor_bump
+cudaError_t launch_dense_rho(const Dev& D, int p_idx, cudaStream_t s);   // rho = row p_idx of B^-1
+cudaError_t launch_ftran_dense(const Dev& D, int check, int force, cudaStream_t s);
+cudaError_t launch_binv_update(const Dev& D, int force, cudaStream_t s);
+cudaError_t launch_dense_ftran_vec(const Dev& D, const double* v, double* y, cudaStream_t s);  // y = B^-1 v
+cudaError_t launch_dense_btran_vec(const Dev& D, const double* c, double* y, cudaStream_t s);  // y = B^-T c
+cudaError_t launch_dense_beta(const Dev& D, cudaStream_t s);             // exact DSE weights
 
 }  // namespace ds

@@ -13,13 +13,23 @@ from parallel_ds_b200 import solver as S
 
 pytestmark = pytest.mark.gpu
 
+# Every test runs with the eta file (PFI, the reference's representation) and with
+# the explicit dense inverse (the default for m <= 4096).
+MODE = {"dense_max_m": 4096}
+
+
+@pytest.fixture(autouse=True, params=["eta", "dense"])
+def linalg_mode(request):
+    MODE["dense_max_m"] = 0 if request.param == "eta" else 4096
+    yield
+
 
 def solve_typed_gpu(t, **opts):
     A = S.Matrix(t["val"], t["row_ptr"], t["col_idx"], t["m"], t["n"])
     prob = S.Problem(t["col_type"], t["row_type"], t["c"], t["row_lb"], t["row_ub"], t["col_lb"],
                      t["col_ub"], A)
     prob.transformToComputeForm()
-    s = S.CudaDualSimplex(prob, **opts)
+    s = S.CudaDualSimplex(prob, **{**MODE, **opts})
     s.initDualSimplex()
     s.presolve("minInfeas")
     sol = s.solve()
@@ -58,7 +68,7 @@ def check_optimal(lp, res, h):
 @pytest.mark.parametrize("seed", range(10))
 def test_plain_small_vs_oracle_and_highs(seed):
     lp = L.plain_small(seed)
-    res = S.solve_lp(lp)
+    res = S.solve_lp(lp, **MODE)
     h = highs(lp)
     check_optimal(lp, res, h)
     orc = po.solve_typed(L.typed(lp))
@@ -75,7 +85,7 @@ def test_plain_small_trajectory_matches_oracle():
     A = S.Matrix(t["val"], t["row_ptr"], t["col_idx"], t["m"], t["n"])
     prob = S.Problem(t["col_type"], t["row_type"], t["c"], t["row_lb"], t["row_ub"], t["col_lb"],
                      t["col_ub"], A)
-    s = S.CudaDualSimplex(prob)
+    s = S.CudaDualSimplex(prob, **MODE)
     s.set_trace(100000)
     s.initDualSimplex()
     s.solve()
@@ -91,28 +101,28 @@ def test_plain_small_trajectory_matches_oracle():
 @pytest.mark.parametrize("seed", [0, 1])
 def test_learned_size_vs_highs(seed):
     lp = L.learned(seed)
-    res = S.solve_lp(lp)
+    res = S.solve_lp(lp, **MODE)
     check_optimal(lp, res, highs(lp))
 
 
 def test_status_primal_infeasible():
     from test_oracle import _infeasible_variant
     lp = _infeasible_variant(L.plain_small(1))
-    res = S.solve_lp(lp)
+    res = S.solve_lp(lp, **MODE)
     assert res["status"] == "primal_infeasible"
 
 
 def test_status_dual_infeasible():
     from test_oracle import _unbounded_variant
     lp = _unbounded_variant(L.plain_small(2))
-    res = S.solve_lp(lp)
+    res = S.solve_lp(lp, **MODE)
     assert res["status"] == "dual_infeasible"
 
 
 def test_phase1_negative_costs_matches_oracle():
     lp = L.plain_small(4)
     lp["c"] = lp["c"] - 0.3
-    res = S.solve_lp(lp)
+    res = S.solve_lp(lp, **MODE)
     orc = po.solve_typed(L.typed(lp))
     assert res["status"] == orc["status"]
     if orc["status"] == "optimal":
