@@ -81,6 +81,9 @@ typedef struct ds_options {
                                   update it by a rank-1 step per iteration instead of
                                   the eta file; exact DSE weights (default 4096;
                                   0 = always the eta file)                        */
+    int    dense_refactor_interval; /* dense mode: iterations between rebuilds of
+                                  B^-1 from a fresh factorisation (default 400; a
+                                  pivot mismatch rebuilds it at once as well)      */
 } ds_options;
 
 typedef struct ds_stats {

@@ -1081,7 +1081,11 @@ struct Engine {
         invalidate_graph();   // launch parameters may have changed
         const bool want_pd = (opt.pricing == DS_PRICING_LEARNED) || ftr_every > 0;
         std::memset(hc, 0, sizeof(Ctl));
-        hc->max_iter = opt.max_iterations; hc->R = std::min(std::max(opt.refactor_interval, 1), cap - 5);
+        hc->max_iter = opt.max_iterations;
+        // dense mode has no eta file: a rebuild only resets rounding, so it runs on
+        // its own (longer) interval unless the reference's cadence is asked for
+        hc->R = (dense && !opt.strict_reference) ? std::max(opt.dense_refactor_interval, 1)
+                                                 : std::min(std::max(opt.refactor_interval, 1), cap - 5);
         hc->phase = 2; hc->prev_q = -1; hc->ybt_n = -1; hc->trace_cap = trace_cap;
         sync_dev();
         push();
@@ -1198,6 +1202,7 @@ void ds_default_options(ds_options* o) {
     o->learned_mix = 0.05;
     o->learned_pdhg_iters = 4000;
     o->dense_max_m = 4096;
+    o->dense_refactor_interval = 400;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }

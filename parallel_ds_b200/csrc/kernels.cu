@@ -451,8 +451,12 @@ __global__ void k_chuzr(Dev D) {
     __syncthreads();
     if (s_pidx >= 0) {
         if (D.dense) {
-            // rho = B^-T e_p = row p of the explicit inverse
-            for (int r = threadIdx.x; r < D.m; r += BS) D.rho[r] = D.Binv[(size_t)r * D.m + s_pidx];
+            // rho = B^-T e_p = row p of the explicit inverse (strided gather,
+            // unrolled so that the loads of one thread are in flight together)
+            const double* src = D.Binv + s_pidx;
+            const size_t M = D.m;
+#pragma unroll 8
+            for (int r = threadIdx.x; r < D.m; r += BS) D.rho[r] = src[(size_t)r * M];
         } else {
             btran_unit_eta<BS>(D, s_pidx, Gs);
         }
