@@ -84,6 +84,9 @@ typedef struct ds_options {
     int    dense_refactor_interval; /* dense mode: iterations between rebuilds of
                                   B^-1 from a fresh factorisation (default 400; a
                                   pivot mismatch rebuilds it at once as well)      */
+    int    learned_start_iteration; /* learned pricing: iterations before this one use
+                                  DSE while the PDHG warm start runs on a second
+                                  stream (default -1 = m/8; 0 = wait for it first) */
 } ds_options;
 
 typedef struct ds_stats {

@@ -133,6 +133,14 @@ struct Engine {
     cudaGraphExec_t pd_gexec = nullptr;
     static constexpr int PDHG_RESTART = 500;
     cudaEvent_t evp0 = nullptr, evp1 = nullptr;
+    // The PDHG warm start runs on its own stream, overlapping the start of the
+    // solve; the main stream waits for it (pd_done) only before the first
+    // iteration the network prices (learn_start), so the pivot sequence does not
+    // depend on timing.
+    cudaStream_t pd_stream = nullptr;
+    cudaEvent_t pd_done = nullptr, pd_go = nullptr;
+    bool pd_pending = false;
+    int learn_start = 0;
     DBuf<int> d_row_nnz, d_enter_cnt, d_entered_at, d_ftr_meta;
 
     Ctl* hc = nullptr;          // pinned host mirror of Ctl
@@ -176,6 +184,9 @@ struct Engine {
         keep_pool_memory(opt.device);
         CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
         CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
+        CK(cudaStreamCreateWithFlags(&pd_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&pd_done, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&pd_go, cudaEventDisableTiming));
         CK(cudaEventCreate(&evr0)); CK(cudaEventCreate(&evr1));
     }
     ~Engine() {
@@ -184,6 +195,9 @@ struct Engine {
         if (ev0) cudaEventDestroy(ev0);
         if (evp0) cudaEventDestroy(evp0);
         if (evp1) cudaEventDestroy(evp1);
+        if (pd_done) cudaEventDestroy(pd_done);
+        if (pd_go) cudaEventDestroy(pd_go);
+        if (pd_stream) cudaStreamDestroy(pd_stream);
         if (pd_gexec) cudaGraphExecDestroy(pd_gexec);
         if (ev1) cudaEventDestroy(ev1);
         if (evr0) cudaEventDestroy(evr0);
@@ -314,27 +328,28 @@ struct Engine {
 
     // ceil(iters / PDHG_RESTART) restart periods of PDHG from the zero start,
     // then the per-variable evidence arrays.
-    void run_pdhg(int iters) {
+    void run_pdhg(int iters) { run_pdhg_on(iters, stream); }
+    void run_pdhg_on(int iters, cudaStream_t ps) {
         PD = PdhgDev{m, n, PDHG_RESTART, d_cptr.p, d_crow.p, d_cval.p, d_rptr.p, d_rcol.p, d_rval.p,
                      d_pd_c.p, d_pd_lo.p, d_pd_hi.p, d_pd_L.p, d_pd_U.p, d_pd_tau.p, d_pd_sigma.p,
                      d_pd_x.p, d_pd_xbar.p, d_pd_xsum.p, d_pd_y.p, d_pd_ysum.p};
-        CK(launch_pdhg_init(PD, stream));
+        CK(launch_pdhg_init(PD, ps));
         if (!pd_gexec) {
             cudaGraph_t g;
-            CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            CK(cudaStreamBeginCapture(ps, cudaStreamCaptureModeThreadLocal));
             set_launch_counting(false);
-            cudaError_t le = launch_pdhg_period(PD, stream);
+            cudaError_t le = launch_pdhg_period(PD, ps);
             set_launch_counting(true);
-            cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            cudaError_t ce = cudaStreamEndCapture(ps, &g);
             CK(le); CK(ce);
             CK(cudaGraphInstantiate(&pd_gexec, g, 0));
             cudaGraphDestroy(g);
         }
         const int periods = (iters + PDHG_RESTART - 1) / PDHG_RESTART;
-        for (int p = 0; p < periods; ++p) CK(cudaGraphLaunch(pd_gexec, stream));
+        for (int p = 0; p < periods; ++p) CK(cudaGraphLaunch(pd_gexec, ps));
         count_launch(periods * 2 * PDHG_RESTART);
-        CK(launch_pdhg_finish(PD, stream));
-        CK(launch_pdhg_evidence(PD, d_pd_gap.p, d_pd_dual.p, stream));
+        CK(launch_pdhg_finish(PD, ps));
+        CK(launch_pdhg_evidence(PD, d_pd_gap.p, d_pd_dual.p, ps));
     }
 
     void pdhg_estimate(int iters, double* x, double* y) {
@@ -342,6 +357,15 @@ struct Engine {
         CK(cudaMemcpyAsync(x, d_pd_x.p, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
         CK(cudaMemcpyAsync(y, d_pd_y.p, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
         CK(cudaStreamSynchronize(stream));
+    }
+
+    // Make the main stream wait for the PDHG evidence before launches whose
+    // iterations reach learn_start.
+    void pd_wait_before(int last_iteration) {
+        if (pd_pending && last_iteration >= learn_start) {
+            CK(cudaStreamWaitEvent(stream, pd_done, 0));
+            pd_pending = false;
+        }
     }
 
     void sync_dev() {
@@ -368,6 +392,7 @@ struct Engine {
         D.learned = (opt.pricing == DS_PRICING_LEARNED && mlp) ? 1 : 0;
         D.learn_mix = opt.learned_mix;
         D.learn_margin = opt.learned_margin;
+        D.learn_start = learn_start;
         D.mlp_w1 = D.mlp_w2 = nullptr; D.mlp_p = nullptr; D.mlp_err = nullptr;
         if (mlp) model_pointers(mlp, &D.mlp_w1, &D.mlp_w2, &D.mlp_p, &D.mlp_err);
         D.score = d_score.p; D.row_nnz = d_row_nnz.p;
@@ -734,7 +759,7 @@ struct Engine {
             case S_BTRAN_RHS: return 24.0 * nnz_S + 20 * K;
             case S_BTRAN_GEMV: return 8 * K * K + 8 * K + 12 * M;
             case S_PIVOT_ROW: return 12.0 * ((double)h_rptr[m] - nnz_S) + 8 * K + 4 * Nn + 8 * (Nn - K) + 8 * M + 50 * Nn;
-            case S_DUAL_UPDATE: return 30 * Nn;
+            case S_DUAL_UPDATE: return 30 * Nn + (dense ? (12.0 + 8 * M) * ((double)h_rptr[m] / n) + 8 * M : 0.0);
             case S_FTRAN_K: return 8 * K * K + 16 * R * K + 8 * R * K * D.ftr_nchunk;
             case S_FTRAN_ASM: return 20.0 * nnz_cpl + (M - K) * (4 + 16 * R) + 8 * R * Tt;
             case S_ETA_APPLY: return 8 * Tt * M + 16 * R * M;
@@ -838,6 +863,7 @@ struct Engine {
                 CK(cudaStreamSynchronize(stream));
             }
             const int T0 = hc->T;
+            pd_wait_before(hc->iteration + 1);
             bool ran[S_NSTEPS] = {};
             for (int stp = 0; stp < S_NSTEPS; ++stp) {
                 if (!step_active(D, stp)) continue;
@@ -870,6 +896,7 @@ struct Engine {
             int batch = R - (it % R);
             if (batch > BATCH_ITERS) batch = BATCH_ITERS;
             if (batch < 1) batch = 1;
+            pd_wait_before(it + batch);
             for (int b = 0; b < batch; ++b) CK(cudaGraphLaunch(gexec, stream));
             count_launch((int)(batch * graph_nodes));
             pull();
@@ -905,6 +932,7 @@ struct Engine {
             CK(cudaStreamSynchronize(stream));
             debug_check_x("before-body");
         }
+        pd_wait_before(hc->iteration);
         CK(launch_body(D, ST_PRICING, stream));
         pull();
         if (opt.verbose >= 3 && !hc->halt) {
@@ -1080,6 +1108,9 @@ struct Engine {
         }
         invalidate_graph();   // launch parameters may have changed
         const bool want_pd = (opt.pricing == DS_PRICING_LEARNED) || ftr_every > 0;
+        learn_start = 0;
+        if (opt.pricing == DS_PRICING_LEARNED && ftr_every == 0)
+            learn_start = opt.learned_start_iteration >= 0 ? opt.learned_start_iteration : m / 8;
         std::memset(hc, 0, sizeof(Ctl));
         hc->max_iter = opt.max_iterations;
         // dense mode has no eta file: a rebuild only resets rounding, so it runs on
@@ -1091,14 +1122,23 @@ struct Engine {
         push();
         const long long launches0 = launch_count();
         CK(cudaEventRecord(ev0, stream));
-        CK(cudaEventRecord(evp0, stream));
+        pd_pending = false;
         if (want_pd && opt.learned_pdhg_iters > 0) {
-            run_pdhg(opt.learned_pdhg_iters);   // warm-start evidence for the scorer's features
+            // warm-start evidence for the scorer's features, on its own stream
+            CK(cudaEventRecord(pd_go, stream));
+            CK(cudaStreamWaitEvent(pd_stream, pd_go, 0));
+            CK(cudaEventRecord(evp0, pd_stream));
+            run_pdhg_on(opt.learned_pdhg_iters, pd_stream);
+            CK(cudaEventRecord(evp1, pd_stream));
+            CK(cudaEventRecord(pd_done, pd_stream));
+            pd_pending = true;
+            if (learn_start == 0) { CK(cudaStreamWaitEvent(stream, pd_done, 0)); pd_pending = false; }
         } else {
+            CK(cudaEventRecord(evp0, stream));
             CK(cudaMemsetAsync(d_pd_gap.p, 0, sizeof(float) * N, stream));
             CK(cudaMemsetAsync(d_pd_dual.p, 0, sizeof(float) * N, stream));
+            CK(cudaEventRecord(evp1, stream));
         }
-        CK(cudaEventRecord(evp1, stream));
         try {
             refactor();                      // initDualSimplex (cudaDualSimplex.cpp:20-81)
             if (perturb_needed()) perturb();  // presolve (tpp:5-30)
@@ -1130,6 +1170,7 @@ struct Engine {
                 if (e.code == DS_ERR_CUDA) throw;
             }
         }
+        if (pd_pending) { CK(cudaStreamWaitEvent(stream, pd_done, 0)); pd_pending = false; }   // count all launched work
         CK(cudaEventRecord(ev1, stream));
         CK(cudaStreamSynchronize(stream));
         float ms = 0; cudaEventElapsedTime(&ms, ev0, ev1);
@@ -1203,6 +1244,7 @@ void ds_default_options(ds_options* o) {
     o->learned_pdhg_iters = 4000;
     o->dense_max_m = 4096;
     o->dense_refactor_interval = 400;
+    o->learned_start_iteration = -1;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }

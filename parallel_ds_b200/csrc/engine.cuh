@@ -128,6 +128,7 @@ struct Dev {
     double* trace_d;    // 2 * trace_cap doubles (theta, obj)
     // learned pricing (mlp.cu)
     int learned;                // 1: CHUZR ranks rows by DSE weight x network score
+    int learn_start;            // first iteration priced by the network (DSE before it)
     double learn_mix;           // score = w * (mix + (1 - mix) * sigmoid(logit))
     double learn_margin;        // minimum sigmoid(logit) of the network's row
     const void* mlp_w1;         // bf16 W1 (64 x 12), row major

@@ -329,7 +329,7 @@ __global__ void k_chuzr(Dev D) {
         }
     }
     const int i = blockIdx.x * BS + threadIdx.x;
-    const bool learned = D.learned && phase == 2;
+    const bool learned = D.learned && phase == 2 && it >= D.learn_start;
     ArgMax best{-1.0, INT_MAX};
     ArgMax bestL{-1.0, INT_MAX};   // learned ranking: DSE weight x network score
     int infeas = 0, dbad = 0;
@@ -751,9 +751,29 @@ __global__ void k_dual_update(Dev D) {
         D.flip[i] = fl;
         nf = fl ? 1 : 0;
     }
+    if (D.dense && i < D.m) {
+        // dense mode: the iteration FTRAN alpha_q = B^-1 a_q rides on this grid
+        const int q = c->q;
+        const size_t M = D.m;
+        double sq = 0.0;
+        if (q < D.n) {
+#pragma unroll 4
+            for (int e = D.cptr[q]; e < D.cptr[q + 1]; ++e) sq += D.Binv[(size_t)D.crow[e] * M + i] * D.cval[e];
+        } else {
+            sq = D.Binv[(size_t)(q - D.n) * M + i];
+        }
+        D.alpha_q[i] = sq;
+    }
     nf = block_sum_int<BS>(nf);
     if (threadIdx.x == 0) D.redi[blockIdx.x] = nf;
     if (!last_block(&c->tickets[4])) return;
+    if (D.dense && threadIdx.x == 0) {
+        // the reference's FTRAN/BTRAN pivot check (cudaDualSimplex.cpp:555)
+        const double aqp = __ldcg(&D.alpha_q[c->p_idx]);
+        const double apq = D.alpha[c->q_idx];
+        if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
+        else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
+    }
     __shared__ int s_nf;
     int tot = 0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += __ldcg(&D.redi[b]);
@@ -1006,7 +1026,20 @@ __global__ void k_update(Dev D, int force) {
         const double aqi = D.alpha_q[i];
         if (phase == 2) {
             double xj = D.x[j];
-            if (nflips > 0) { const double dx = D.dxb[i]; xj = xj - dx; dzc = D.cost[j] * dx; }
+            if (nflips > 0) {
+                double dx;
+                if (D.dense) {   // dx_B = B^-1 column_change (bound flips, rare)
+                    dx = 0.0;
+                    for (int r = 0; r < D.m; ++r) {
+                        const double v = D.cc[r];
+                        if (v != 0.0) dx += D.Binv[(size_t)r * D.m + i] * v;
+                    }
+                } else {
+                    dx = D.dxb[i];
+                }
+                xj = xj - dx;
+                dzc = D.cost[j] * dx;
+            }
             xj = xj - theta_P * aqi;
             D.x[j] = xj;
         } else if (i != p_idx) {
@@ -1335,7 +1368,8 @@ bool step_active(const Dev& D, int step) {
         case S_SCORE: return score_step_active(D);
         case S_BTRAN_RHS: case S_FTRAN_K: return !D.dense && D.k > 0;
         case S_BTRAN_GEMV: case S_FTRAN_ASM: case S_ETA_APPLY: return !D.dense;
-        case S_FTRAN_DENSE: case S_BINV: return D.dense != 0;
+        case S_FTRAN_DENSE: return false;   // dense FTRAN runs inside k_dual_update (mismatch path: launch_ftran_dense)
+        case S_BINV: return D.dense != 0;
         default: return true;
     }
 }
@@ -1378,7 +1412,7 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
             break;
         }
         case S_PIVOT_ROW: k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, 3); break;
-        case S_DUAL_UPDATE: k_dual_update<BS><<<nblk(D.n), BS, 0, s>>>(D); break;
+        case S_DUAL_UPDATE: k_dual_update<BS><<<nblk(D.dense && D.m > D.n ? D.m : D.n), BS, 0, s>>>(D); break;
         case S_FTRAN_K:
             if (D.k > 0) {
                 dim3 g(D.ftr_ntile, D.ftr_nchunk);

@@ -126,9 +126,20 @@ __device__ __forceinline__ uint32_t kofs(int r, int k, uint32_t kblock_bytes) {
 __device__ __forceinline__ void st_bf16(unsigned char* base, uint32_t off, float v) {
     *reinterpret_cast<__nv_bfloat16*>(base + off) = __float2bfloat16_rn(v);
 }
+// Eight consecutive K elements of one row are one 16-byte core-matrix row.
+__device__ __forceinline__ void st_bf16x8(unsigned char* base, uint32_t off, const float* v) {
+    uint4 u;
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(v[0], v[1]), p1 = __floats2bfloat162_rn(v[2], v[3]);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(v[4], v[5]), p3 = __floats2bfloat162_rn(v[6], v[7]);
+    u.x = *reinterpret_cast<uint32_t*>(&p0); u.y = *reinterpret_cast<uint32_t*>(&p1);
+    u.z = *reinterpret_cast<uint32_t*>(&p2); u.w = *reinterpret_cast<uint32_t*>(&p3);
+    *reinterpret_cast<uint4*>(base + off) = u;
+}
 
 // --------------------------------------------------------------- parameters
-// fp32 master layout (DS_MLP_NPARAMS floats): W1[64][12], b1[64], W2[64][64], b2[64], w3[64], b3
+// fp32 master layout (DS_MLP_NPARAMS floats): W1[64][12], b1[64], W2[64][64], b2[64], w3[64], b3.
+// The bf16 copies the MMAs read: W1 padded to [64][16] (zero columns 12..15) and W2
+// [64][64], so that every row is a whole number of 16-byte core-matrix rows.
 constexpr int NF = DS_NUM_FEATURES;
 constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + 64 * NF, OFF_W2 = OFF_B1 + 64, OFF_B2 = OFF_W2 + 64 * 64,
               OFF_W3 = OFF_B2 + 64, OFF_B3 = OFF_W3 + 64, NPARAMS = OFF_B3 + 1;
@@ -215,9 +226,19 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
         const Ctl* c = D.ctl;
         if (*(volatile const int*)&c->halt || c->phase != 2) return;   // block-uniform
         it = pricing_iteration(c);
+        if (it < D.learn_start) return;   // DSE prices these iterations; no scores needed
     }
+    __shared__ float sP[3 * 64 + 1];                             // b1, b2, w3, b3
     if (tid == 0) { mbar_init(&mbar, 1); bad = 0; }
     if (warp == 0) tmem_alloc(&tmem_base, 128);
+    // weights first (independent of the features): 16-byte loads straight into
+    // the K-major core-matrix layout
+    *reinterpret_cast<uint4*>(sB1 + kofs(tid >> 1, 8 * (tid & 1), KB_B)) = reinterpret_cast<const uint4*>(a.W1b)[tid];
+#pragma unroll
+    for (int c = tid; c < 512; c += 128)
+        *reinterpret_cast<uint4*>(sB2 + kofs(c >> 3, 8 * (c & 7), KB_B)) = reinterpret_cast<const uint4*>(a.W2b)[c];
+    for (int e = tid; e < 3 * 64 + 1; e += 128)   // w3 and b3 are adjacent (OFF_W3 + 64 == OFF_B3)
+        sP[e] = e < 64 ? a.P[OFF_B1 + e] : e < 128 ? a.P[OFF_B2 + e - 64] : a.P[OFF_W3 + e - 128];
     float f[16];
     bool cand = false;
     if (live) {
@@ -231,16 +252,8 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
     } else {
         for (int k = 0; k < 16; ++k) f[k] = 0.f;
     }
-    for (int k = 0; k < 16; ++k) st_bf16(sA1, kofs(tid, k, KB_A), f[k]);
-    for (int e = tid; e < 64 * 16; e += 128) {
-        const int o = e >> 4, k = e & 15;
-        *reinterpret_cast<__nv_bfloat16*>(sB1 + kofs(o, k, KB_B)) =
-            (k < NF) ? a.W1b[o * NF + k] : __float2bfloat16_rn(0.f);
-    }
-    for (int e = tid; e < 64 * 64; e += 128) {
-        const int o = e >> 6, k = e & 63;
-        *reinterpret_cast<__nv_bfloat16*>(sB2 + kofs(o, k, KB_B)) = a.W2b[o * 64 + k];
-    }
+    st_bf16x8(sA1, kofs(tid, 0, KB_A), f);
+    st_bf16x8(sA1, kofs(tid, 8, KB_A), f + 8);
     fence_async_smem();
     tc_before_sync();
     __syncthreads();
@@ -255,10 +268,10 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
     tc_after_sync();
     float h[64];
     tmem_ld64(tm + lane_base, h);
-    for (int k = 0; k < 64; ++k) {
-        h[k] = fmaxf(h[k] + a.P[OFF_B1 + k], 0.f);
-        st_bf16(sA2, kofs(tid, k, KB_A), h[k]);
-    }
+#pragma unroll
+    for (int k = 0; k < 64; ++k) h[k] = fmaxf(h[k] + sP[k], 0.f);
+#pragma unroll
+    for (int c8 = 0; c8 < 8; ++c8) st_bf16x8(sA2, kofs(tid, 8 * c8, KB_A), h + 8 * c8);
     if (live && a.H1) for (int k = 0; k < 64; ++k) a.H1[(size_t)row * 64 + k] = h[k];
     fence_async_smem();
     tc_before_sync();
@@ -273,10 +286,10 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
     if (!mbar_wait(&mbar, 1)) bad = 1;
     tc_after_sync();
     tmem_ld64(tm + lane_base + 64, h);
-    float logit = a.P[OFF_B3];
+    float logit = sP[192];
     for (int k = 0; k < 64; ++k) {
-        h[k] = fmaxf(h[k] + a.P[OFF_B2 + k], 0.f);
-        logit += h[k] * a.P[OFF_W3 + k];
+        h[k] = fmaxf(h[k] + sP[64 + k], 0.f);
+        logit += h[k] * sP[128 + k];
     }
     if (live && a.H2) for (int k = 0; k < 64; ++k) a.H2[(size_t)row * 64 + k] = h[k];
     if (live) {
@@ -471,13 +484,13 @@ __global__ void k_mlp_adam(float* P, float* m1, float* m2, const float* g, float
     const float vh = a2 / (1.f - powf(b2, (float)step));
     const float v = P[p] - lr * mh / (sqrtf(vh) + eps);
     P[p] = v;
-    if (p < OFF_B1) W1b[p] = __float2bfloat16_rn(v);
+    if (p < OFF_B1) W1b[(p / NF) * 16 + p % NF] = __float2bfloat16_rn(v);
     else if (p >= OFF_W2 && p < OFF_B2) W2b[p - OFF_W2] = __float2bfloat16_rn(v);
 }
 
 __global__ void k_mlp_to_bf16(const float* P, __nv_bfloat16* W1b, __nv_bfloat16* W2b) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p < 64 * NF) W1b[p] = __float2bfloat16_rn(P[OFF_W1 + p]);
+    if (p < 64 * 16) W1b[p] = __float2bfloat16_rn((p % 16) < NF ? P[OFF_W1 + (p / 16) * NF + p % 16] : 0.f);
     if (p < 64 * 64) W2b[p] = __float2bfloat16_rn(P[OFF_W2 + p]);
 }
 
@@ -619,14 +632,14 @@ int ds_model_create(int device, ds_model** out) {
     ok = ok && cudaMalloc(&md->m2, ds::NPARAMS * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&md->g, ds::NPARAMS * sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&md->loss, sizeof(float)) == cudaSuccess;
-    ok = ok && cudaMalloc(&md->W1b, 64 * ds::NF * sizeof(__nv_bfloat16)) == cudaSuccess;
+    ok = ok && cudaMalloc(&md->W1b, 64 * 16 * sizeof(__nv_bfloat16)) == cudaSuccess;
     ok = ok && cudaMalloc(&md->W2b, 64 * 64 * sizeof(__nv_bfloat16)) == cudaSuccess;
     ok = ok && cudaMalloc(&md->err, sizeof(int)) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->P, 0, ds::NPARAMS * sizeof(float), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->m1, 0, ds::NPARAMS * sizeof(float), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->m2, 0, ds::NPARAMS * sizeof(float), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->err, 0, sizeof(int), md->stream) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(md->W1b, 0, 64 * ds::NF * sizeof(__nv_bfloat16), md->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(md->W1b, 0, 64 * 16 * sizeof(__nv_bfloat16), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->W2b, 0, 64 * 64 * sizeof(__nv_bfloat16), md->stream) == cudaSuccess;
     ok = ok && cudaStreamSynchronize(md->stream) == cudaSuccess;
     if (!ok) { delete md; return DS_ERR_CUDA; }
