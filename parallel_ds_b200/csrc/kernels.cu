@@ -309,6 +309,111 @@ __device__ void btran_unit_eta(const Dev& D, int p_idx, double* Gs) {
 // then DSEPricing (tpp:470-501) + checkPrimalFeasible (tpp:296-324), or
 // phase1Pricing (tpp:746-772) when Ctl::phase == 1.  Threads cover max(m, n):
 // positions for pricing, nonbasic slots for the dual check.
+// Loop bookkeeping at the top of the reference's iteration (cudaDualSimplex.cpp:419-446).
+__device__ __forceinline__ void chuzr_top(const Ctl* c, bool do_top, int* it, int* top_ev, bool* dual_chk) {
+    *it = c->iteration;
+    *top_ev = EV_NONE;
+    *dual_chk = false;
+    if (do_top) {
+        *it += 1;
+        if (*it > c->max_iter) *top_ev = EV_ITER_LIMIT;
+        else if (*it % c->R == 0) *top_ev = EV_REFACTOR_DUE;
+        else {
+            *dual_chk = (*it % NEED_RESTART == 0);
+            if (!*dual_chk && !c->perturbed && c->cycle > MAX_CYCLE) *top_ev = EV_PERTURB;
+        }
+    }
+}
+
+// One basis position of DSEPricing (phase 2) or phase1Pricing (phase 1).
+__device__ __forceinline__ void chuzr_row(const Dev& D, int i, int phase, bool learned, ArgMax& best, ArgMax& bestL,
+                                          int& infeas) {
+    const int j = D.basis[i];
+    const unsigned char t = D.type[j];
+    if (phase == 2) {
+        const double x = D.x[j], l = D.lb[j], u = D.ub[j];
+        double dt;
+        if (var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8) {
+            const double w = (dt * dt) / D.beta[i];
+            if (w > 0.0) {
+                best = better_max(best, ArgMax{w, i});   // strict '>' against max_weight = 0; NaN never wins
+                if (learned) {
+                    const double sg = 1.0 / (1.0 + exp(-(double)D.score[i]));
+                    const double v = w * (D.learn_mix + (1.0 - D.learn_mix) * sg);
+                    if (v > 0.0) bestL = better_max(bestL, ArgMax{v, i});
+                }
+            }
+        }
+        infeas += var_primal_ok(t, x, l, u) ? 0 : 1;
+    } else {
+        const double fi = D.f[i];
+        if ((t == LOWER && fi > EPS_F) || (t == UPPER && fi < -EPS_F) || t == BOXED || t == FIXED) {
+            const double w = (fi * fi) / D.beta[i];
+            if (w > 0.0 && !D.blocked[j]) best = better_max(best, ArgMax{w, i});
+        }
+    }
+}
+
+// Thread 0's decision after the reductions of CHUZR: loop bookkeeping events,
+// the dual check, the optimality test, the leaving row (DSE or learned) or the
+// phase-1 outcome.  Returns the leaving position for the eta part of BTRAN, or -1.
+__device__ int chuzr_decide(const Dev& D, Ctl* c, ArgMax v, ArgMax vL, int tot, int dtot, int top_ev, bool dual_chk,
+                            bool do_top, int it, bool learned, int phase) {
+    int s_pidx = -1;
+    if (do_top) c->iteration = it;
+    c->top_done = 0;
+    int pidx = (v.i == INT_MAX || v.w <= 0.0) ? -1 : v.i;
+    // Learned pricing: take the network's row when it is a valid leaving
+    // row (a primal infeasible position) whose sigmoid score reaches the
+    // margin; otherwise fall back to the DSE row.
+    if (learned && top_ev == EV_NONE && !(dual_chk && dtot > 0) && pidx >= 0) {
+        const int pl = (vL.i == INT_MAX || !(vL.w > 0.0)) ? -1 : vL.i;
+        const double sg = pl >= 0 ? 1.0 / (1.0 + exp(-(double)D.score[pl])) : 0.0;
+        if (pl >= 0 && sg >= D.learn_margin) { pidx = pl; c->learned_used += 1; }
+        else c->learned_fallback += 1;
+    }
+    if (top_ev != EV_NONE) {
+        raise_ev(c, top_ev, ST_TOP);
+    } else if (dual_chk && dtot > 0) {
+        raise_ev(c, EV_DUALINF, ST_TOP);
+    } else if (dual_chk && !c->perturbed && c->cycle > MAX_CYCLE) {
+        raise_ev(c, EV_PERTURB, ST_TOP);
+    } else if (phase == 2) {
+        c->primal_feasible = (tot == 0);
+        c->ninfeas = tot;
+        c->p = -1; c->p_idx = -1;
+        if (pidx >= 0) {
+            const int j = D.basis[pidx];
+            double dt;
+            var_infeas(D.type[j], D.x[j], D.lb[j], D.ub[j], &dt);
+            c->p = j; c->p_idx = pidx; c->delta = dt; c->is_lower = dt < 0;
+            c->beta_p = D.beta[pidx];
+        }
+        if (tot == 0) raise_ev(c, EV_OPTIMAL, ST_PRICING);
+        else if (pidx < 0) raise_ev(c, EV_NO_P, ST_PRICING);
+        else s_pidx = pidx;
+    } else {
+        const int found = pidx >= 0;
+        c->p1_found = found;
+        const int dinf = c->p1_dinf;
+        const double Z = c->z_phase1;
+        int ev = EV_NONE;
+        if (!found || !dinf) {
+            if (fabs(Z) < EPS_A || !dinf) ev = EV_P1_DONE;
+            else if (Z > 0) ev = EV_P1_DUALINF;
+        }
+        if (ev == EV_NONE && pidx < 0) ev = EV_P1_RESTART;
+        if (ev == EV_NONE && Z > EPS_BOUND) ev = EV_P1_RESTART;
+        if (ev != EV_NONE) raise_ev(c, ev, ST_PRICING);
+        else {
+            c->p = D.basis[pidx]; c->p_idx = pidx; c->f_p = D.f[pidx];
+            c->beta_p = D.beta[pidx];
+            s_pidx = pidx;
+        }
+    }
+    return s_pidx;
+}
+
 template <int BS>
 __global__ void k_chuzr(Dev D) {
     extern __shared__ double Gs[];
@@ -316,54 +421,17 @@ __global__ void k_chuzr(Dev D) {
     if (halted(c)) return;
     const int phase = c->phase;
     const bool do_top = (phase == 2 && !c->top_done);
-    int it = c->iteration;
-    int top_ev = EV_NONE;
-    bool dual_chk = false;
-    if (do_top) {
-        it += 1;
-        if (it > c->max_iter) top_ev = EV_ITER_LIMIT;
-        else if (it % c->R == 0) top_ev = EV_REFACTOR_DUE;
-        else {
-            dual_chk = (it % NEED_RESTART == 0);
-            if (!dual_chk && !c->perturbed && c->cycle > MAX_CYCLE) top_ev = EV_PERTURB;
-        }
-    }
+    int it, top_ev;
+    bool dual_chk;
+    chuzr_top(c, do_top, &it, &top_ev, &dual_chk);
     const int i = blockIdx.x * BS + threadIdx.x;
     const bool learned = D.learned && phase == 2 && it >= D.learn_start;
     ArgMax best{-1.0, INT_MAX};
     ArgMax bestL{-1.0, INT_MAX};   // learned ranking: DSE weight x network score
     int infeas = 0, dbad = 0;
     if (top_ev == EV_NONE) {
-        if (i < D.m) {
-            const int j = D.basis[i];
-            const unsigned char t = D.type[j];
-            if (phase == 2) {
-                const double x = D.x[j], l = D.lb[j], u = D.ub[j];
-                double dt;
-                if (var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8) {
-                    const double w = (dt * dt) / D.beta[i];
-                    if (w > 0.0) {
-                        best = ArgMax{w, i};   // strict '>' against max_weight = 0; NaN never wins
-                        if (learned) {
-                            const double sg = 1.0 / (1.0 + exp(-(double)D.score[i]));
-                            const double v = w * (D.learn_mix + (1.0 - D.learn_mix) * sg);
-                            if (v > 0.0) bestL = ArgMax{v, i};
-                        }
-                    }
-                }
-                infeas = var_primal_ok(t, x, l, u) ? 0 : 1;
-            } else {
-                const double fi = D.f[i];
-                if ((t == LOWER && fi > EPS_F) || (t == UPPER && fi < -EPS_F) || t == BOXED || t == FIXED) {
-                    const double w = (fi * fi) / D.beta[i];
-                    if (w > 0.0 && !D.blocked[j]) best = ArgMax{w, i};
-                }
-            }
-        }
-        if (dual_chk && i < D.n) {
-            const int j = D.nonbasis[i];
-            dbad = var_dual_bad(D.type[j], D.d[j]) ? 1 : 0;
-        }
+        if (i < D.m) chuzr_row(D, i, phase, learned, best, bestL, infeas);
+        if (dual_chk && i < D.n) dbad = var_dual_bad(D.type[D.nonbasis[i]], D.d[D.nonbasis[i]]) ? 1 : 0;
     }
     best = block_argmax<BS>(best);
     if (learned) bestL = block_argmax<BS>(bestL);
@@ -394,60 +462,8 @@ __global__ void k_chuzr(Dev D) {
     if (learned) vL = block_argmax<BS>(vL);
     tot = block_sum_int<BS>(tot);
     dtot = block_sum_int<BS>(dtot);
-    if (threadIdx.x == 0) {
-        s_pidx = -1;
-        if (do_top) c->iteration = it;
-        c->top_done = 0;
-        int pidx = (v.i == INT_MAX || v.w <= 0.0) ? -1 : v.i;
-        // Learned pricing: take the network's row when it is a valid leaving
-        // row (a primal infeasible position) whose sigmoid score reaches the
-        // margin; otherwise fall back to the DSE row.
-        if (learned && top_ev == EV_NONE && !(dual_chk && dtot > 0) && pidx >= 0) {
-            const int pl = (vL.i == INT_MAX || !(vL.w > 0.0)) ? -1 : vL.i;
-            const double sg = pl >= 0 ? 1.0 / (1.0 + exp(-(double)D.score[pl])) : 0.0;
-            if (pl >= 0 && sg >= D.learn_margin) { pidx = pl; c->learned_used += 1; }
-            else c->learned_fallback += 1;
-        }
-        if (top_ev != EV_NONE) {
-            raise_ev(c, top_ev, ST_TOP);
-        } else if (dual_chk && dtot > 0) {
-            raise_ev(c, EV_DUALINF, ST_TOP);
-        } else if (dual_chk && !c->perturbed && c->cycle > MAX_CYCLE) {
-            raise_ev(c, EV_PERTURB, ST_TOP);
-        } else if (phase == 2) {
-            c->primal_feasible = (tot == 0);
-            c->ninfeas = tot;
-            c->p = -1; c->p_idx = -1;
-            if (pidx >= 0) {
-                const int j = D.basis[pidx];
-                double dt;
-                var_infeas(D.type[j], D.x[j], D.lb[j], D.ub[j], &dt);
-                c->p = j; c->p_idx = pidx; c->delta = dt; c->is_lower = dt < 0;
-                c->beta_p = D.beta[pidx];
-            }
-            if (tot == 0) raise_ev(c, EV_OPTIMAL, ST_PRICING);
-            else if (pidx < 0) raise_ev(c, EV_NO_P, ST_PRICING);
-            else s_pidx = pidx;
-        } else {
-            const int found = pidx >= 0;
-            c->p1_found = found;
-            const int dinf = c->p1_dinf;
-            const double Z = c->z_phase1;
-            int ev = EV_NONE;
-            if (!found || !dinf) {
-                if (fabs(Z) < EPS_A || !dinf) ev = EV_P1_DONE;
-                else if (Z > 0) ev = EV_P1_DUALINF;
-            }
-            if (ev == EV_NONE && pidx < 0) ev = EV_P1_RESTART;
-            if (ev == EV_NONE && Z > EPS_BOUND) ev = EV_P1_RESTART;
-            if (ev != EV_NONE) raise_ev(c, ev, ST_PRICING);
-            else {
-                c->p = D.basis[pidx]; c->p_idx = pidx; c->f_p = D.f[pidx];
-                c->beta_p = D.beta[pidx];
-                s_pidx = pidx;
-            }
-        }
-    }
+    if (threadIdx.x == 0)
+        s_pidx = chuzr_decide(D, c, v, vL, tot, dtot, top_ev, dual_chk, do_top, it, learned, phase);
     __syncthreads();
     if (s_pidx >= 0) {
         if (D.dense) {
@@ -460,6 +476,40 @@ __global__ void k_chuzr(Dev D) {
         } else {
             btran_unit_eta<BS>(D, s_pidx, Gs);
         }
+    }
+}
+
+// CHUZR in one CTA (dense mode): every thread scans m / BS positions, so no
+// partials, ticket or second pass; then the gather of rho = row p of B^-1.
+template <int BS>
+__global__ void __launch_bounds__(BS) k_chuzr_cta(Dev D) {
+    Ctl* c = D.ctl;
+    if (halted(c)) return;
+    const int phase = c->phase;
+    const bool do_top = (phase == 2 && !c->top_done);
+    int it, top_ev;
+    bool dual_chk;
+    chuzr_top(c, do_top, &it, &top_ev, &dual_chk);
+    const bool learned = D.learned && phase == 2 && it >= D.learn_start;
+    ArgMax best{-1.0, INT_MAX}, bestL{-1.0, INT_MAX};
+    int infeas = 0, dbad = 0;
+    if (top_ev == EV_NONE) {
+        for (int i = threadIdx.x; i < D.m; i += BS) chuzr_row(D, i, phase, learned, best, bestL, infeas);
+        if (dual_chk)
+            for (int i = threadIdx.x; i < D.n; i += BS) dbad += var_dual_bad(D.type[D.nonbasis[i]], D.d[D.nonbasis[i]]) ? 1 : 0;
+    }
+    best = block_argmax<BS>(best);
+    if (learned) bestL = block_argmax<BS>(bestL);
+    infeas = block_sum_int<BS>(infeas);
+    dbad = block_sum_int<BS>(dbad);
+    __shared__ int s_pidx;
+    if (threadIdx.x == 0) s_pidx = chuzr_decide(D, c, best, bestL, infeas, dbad, top_ev, dual_chk, do_top, it, learned, phase);
+    __syncthreads();
+    if (s_pidx >= 0) {
+        const double* src = D.Binv + s_pidx;
+        const size_t M = D.m;
+#pragma unroll 4
+        for (int r = threadIdx.x; r < D.m; r += BS) D.rho[r] = src[(size_t)r * M];
     }
 }
 
@@ -630,7 +680,21 @@ __global__ void k_pivot_row(Dev D, int mode) {
         double acc = 0.0;
         if (mode & 1) {
             if (j < D.n) {
-                for (int e = D.cptr[j]; e < D.cptr[j + 1]; ++e) acc += D.cval[e] * D.rho[D.crow[e]];
+                // the CSC order of the reference's dot (matrix.cpp:273-286), with the
+                // loads of eight nonzeros issued before their products are summed
+                const int e1 = D.cptr[j + 1];
+                int e = D.cptr[j];
+                for (; e + 8 <= e1; e += 8) {
+                    int rr[8];
+                    double vv[8], pp[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) { rr[u] = D.crow[e + u]; vv[u] = D.cval[e + u]; }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) pp[u] = D.rho[rr[u]];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) acc += vv[u] * pp[u];
+                }
+                for (; e < e1; ++e) acc += D.cval[e] * D.rho[D.crow[e]];
             } else {
                 acc += 1.0 * D.rho[j - D.n];
             }
@@ -1404,7 +1468,10 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
         case S_FTRAN_DENSE: return launch_ftran_dense(D, 1, 0, s);
         case S_BINV: return launch_binv_update(D, 0, s);
         case S_SCORE: return launch_score(D, s);
-        case S_CHUZR: k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D); break;
+        case S_CHUZR:
+            if (D.dense) k_chuzr_cta<1024><<<1, 1024, 0, s>>>(D);
+            else k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D);
+            break;
         case S_BTRAN_RHS: if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, 0); else return cudaSuccess; break;
         case S_BTRAN_GEMV: {
             const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
