@@ -416,6 +416,7 @@ __device__ int chuzr_decide(const Dev& D, Ctl* c, ArgMax v, ArgMax vL, int tot, 
 
 template <int BS>
 __global__ void k_chuzr(Dev D) {
+    pdl_enter();
     extern __shared__ double Gs[];
     Ctl* c = D.ctl;
     if (halted(c)) return;
@@ -483,6 +484,7 @@ __global__ void k_chuzr(Dev D) {
 // partials, ticket or second pass; then the gather of rho = row p of B^-1.
 template <int BS>
 __global__ void __launch_bounds__(BS) k_chuzr_cta(Dev D) {
+    pdl_enter();
     Ctl* c = D.ctl;
     if (halted(c)) return;
     const int phase = c->phase;
@@ -524,6 +526,7 @@ __global__ void k_btran_unit(Dev D, int p_idx) {
 // rhs_j = y[s_pos[j]] - sum_{r in col(s_var[j]), r in R} a_rj * y[slackpos(r)]
 template <int BS>
 __global__ void k_btran_rhs(Dev D, int force) {
+    pdl_enter();
     if (!force && halted(D.ctl)) return;
     const int j = blockIdx.x * BS + threadIdx.x;
     if (j >= D.k) return;
@@ -539,6 +542,7 @@ __global__ void k_btran_rhs(Dev D, int force) {
 // rho[rp_row[t]] = sum_j Kinv(j, t) rhs_j (one warp per t), rho[r] = y[slackpos(r)] for r in R.
 template <int BS>
 __global__ void k_btran_gemv(Dev D, double* out, int force) {
+    pdl_enter();
     if (!force && halted(D.ctl)) return;
     const int warps_per_block = BS / 32;
     const int nb_warp = (D.k + warps_per_block - 1) / warps_per_block;
@@ -668,6 +672,7 @@ __device__ int rt_select(const Dev& D, double sgn_a) {
 // (cudaDualSimplex.cpp:484-549).  Phase 1 uses phase1SetRatioTestCandidates.
 template <int BS>
 __global__ void k_pivot_row(Dev D, int mode) {
+    pdl_enter();
     Ctl* c = D.ctl;
     if (halted(c)) return;
     const int phase = c->phase;
@@ -796,6 +801,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
 // flip list, the column change and delta_z, and the dense entering column.
 template <int BS>
 __global__ void k_dual_update(Dev D) {
+    pdl_enter();
     Ctl* c = D.ctl;
     if (halted(c)) return;
     const int phase = c->phase;
@@ -922,6 +928,7 @@ __device__ bool last_in_tile(unsigned* ticket) {
 
 template <int BS>
 __global__ void k_ftran_k2(Dev D, int nr_fixed, int force) {
+    pdl_enter();
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
     const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
@@ -979,6 +986,7 @@ __global__ void k_ftran_k2(Dev D, int nr_fixed, int force) {
 // last block gathers g_t = y0[p_t] and solves s = Mtri g for the eta chain.
 template <int BS>
 __global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
+    pdl_enter();
     extern __shared__ double Gs[];
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
@@ -1017,6 +1025,7 @@ __global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
 // |alpha_q[p] - alpha_p[q]| > EPS_R (1 + |alpha_q[p]|)  (cudaDualSimplex.cpp:555).
 template <int BS>
 __global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
+    pdl_enter();
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
     const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
@@ -1073,102 +1082,122 @@ __global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
 // ===================================================================== update
 // updateAndChangeBasis (cudaDualSimplex.cpp:254-282) / phase1UpdateAndChangeBasis
 // (:285-309), BFRT x_B correction (:595-617), flips and objective (:618-634).
-template <int BS>
-__global__ void k_update(Dev D, int force) {
-    Ctl* c = D.ctl;
-    if (!force && halted(c)) return;
-    const int phase = c->phase;
-    const int p_idx = c->p_idx, T = c->T;
-    const double ap = D.alpha_q[p_idx];
-    const double bp = c->beta_p;
-    const double theta_P = (phase == 2) ? c->delta_bfrt / ap : c->f_p / ap;
-    const int nflips = c->nflips;
-    const int i = blockIdx.x * BS + threadIdx.x;
+struct UpdArgs {
+    int phase, p_idx, T, nflips;
+    double ap, bp, theta_P;
+};
+__device__ __forceinline__ UpdArgs update_args(const Dev& D, const Ctl* c) {
+    UpdArgs u;
+    u.phase = c->phase; u.p_idx = c->p_idx; u.T = c->T; u.nflips = c->nflips;
+    u.ap = __ldcg(&D.alpha_q[u.p_idx]);
+    u.bp = c->beta_p;
+    u.theta_P = (u.phase == 2) ? c->delta_bfrt / u.ap : c->f_p / u.ap;
+    return u;
+}
+
+// Basis position i: x_B (phase 2) or f (phase 1), and in eta-file mode the new
+// eta entry and the DSE weight.  Returns the objective correction of flips.
+__device__ double update_position(const Dev& D, const UpdArgs& u, int i) {
+    const int j = D.basis[i];
+    const double aqi = D.alpha_q[i];
     double dzc = 0.0;
-    if (i < D.m) {
-        const int j = D.basis[i];
-        const double aqi = D.alpha_q[i];
-        if (phase == 2) {
-            double xj = D.x[j];
-            if (nflips > 0) {
-                double dx;
-                if (D.dense) {   // dx_B = B^-1 column_change (bound flips, rare)
-                    dx = 0.0;
-                    for (int r = 0; r < D.m; ++r) {
-                        const double v = D.cc[r];
-                        if (v != 0.0) dx += D.Binv[(size_t)r * D.m + i] * v;
-                    }
-                } else {
-                    dx = D.dxb[i];
+    if (u.phase == 2) {
+        double xj = D.x[j];
+        if (u.nflips > 0) {
+            double dx;
+            if (D.dense) {   // dx_B = B^-1 column_change (bound flips, rare)
+                dx = 0.0;
+                for (int r = 0; r < D.m; ++r) {
+                    const double v = D.cc[r];
+                    if (v != 0.0) dx += D.Binv[(size_t)r * D.m + i] * v;
                 }
-                xj = xj - dx;
-                dzc = D.cost[j] * dx;
+            } else {
+                dx = D.dxb[i];
             }
-            xj = xj - theta_P * aqi;
-            D.x[j] = xj;
-        } else if (i != p_idx) {
-            D.f[i] = D.f[i] - aqi * theta_P;
+            xj = xj - dx;
+            dzc = D.cost[j] * dx;
         }
-        if (!D.dense) {   // dense mode: B^-1 and exact DSE weights are updated by k_binv_update
-            D.eta[(size_t)T * D.m + i] = (i != p_idx) ? -aqi / ap : 1 / ap;
-            if (i != p_idx) {
-                const double r = aqi / ap;
-                D.beta[i] = D.beta[i] - 2 * aqi / ap * D.tau[i] + (r * r) * bp;
-            }
+        xj = xj - u.theta_P * aqi;
+        D.x[j] = xj;
+    } else if (i != u.p_idx) {
+        D.f[i] = D.f[i] - aqi * u.theta_P;
+    }
+    if (!D.dense) {   // dense mode: B^-1 and exact DSE weights are updated by k_binv_update
+        D.eta[(size_t)u.T * D.m + i] = (i != u.p_idx) ? -aqi / u.ap : 1 / u.ap;
+        if (i != u.p_idx) {
+            const double r = aqi / u.ap;
+            D.beta[i] = D.beta[i] - 2 * aqi / u.ap * D.tau[i] + (r * r) * u.bp;
         }
     }
-    if (phase == 2 && nflips > 0) {
+    return dzc;
+}
+
+// One thread, after every position: objective, entering value, basis swap,
+// flips, cycle counter, trace.  nred: number of flip-objective partials in red.
+__device__ void update_tail(const Dev& D, Ctl* c, const UpdArgs& u, int nred) {
+    const int p = c->p, q = c->q, q_idx = c->q_idx, p_idx = u.p_idx;
+    if (!D.dense) D.beta[p_idx] = u.bp / (u.ap * u.ap);
+    if (u.phase == 2) {
+        double dz = c->dz;
+        if (u.nflips > 0) for (int b = 0; b < nred; ++b) dz -= __ldcg(&D.red[b]);
+        c->obj += dz;
+        D.x[q] = D.x[q] + u.theta_P;
+    } else {
+        D.f[p_idx] = D.f[p_idx] / u.ap + c->dz;   // + infisibilityCorr
+    }
+    D.basis[p_idx] = q;
+    D.nonbasis[q_idx] = p;
+    D.var_pos[q] = p_idx;
+    D.var_pos[p] = -(q_idx + 1);
+    if (D.enter_count) { D.enter_count[q] += 1; D.entered_at[q] = c->iteration; }
+    if (u.phase == 2 && u.nflips > 0) {
+        for (int k = 0; k < D.n; ++k) {
+            const int code = D.flip_list[k];
+            if (k >= u.nflips) break;
+            if (code >= 0) D.x[code] = D.ub[code];
+            else D.x[-code - 1] = D.lb[-code - 1];
+        }
+    }
+    const double theta = c->theta;
+    if (u.phase == 2) {
+        c->obj += theta * c->delta_bfrt;
+        if (fabs(theta) < EPS_A) c->cycle += 1;
+    } else {
+        c->cycle = (fabs(theta) < EPS_A) ? c->cycle + 1 : 0;
+    }
+    if (!D.dense) D.eta_pos[u.T] = p_idx;
+    c->pivots += 1;
+    if (u.phase == 2 && c->trace_n < c->trace_cap) {
+        const int tn = c->trace_n;
+        D.trace[2 * tn] = p; D.trace[2 * tn + 1] = q;
+        D.trace_d[2 * tn] = theta; D.trace_d[2 * tn + 1] = c->obj;
+    }
+    if (u.phase == 2) c->trace_n += 1;
+}
+
+template <int BS>
+__global__ void k_update(Dev D, int force) {
+    pdl_enter();
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const UpdArgs u = update_args(D, c);
+    const int i = blockIdx.x * BS + threadIdx.x;
+    double dzc = 0.0;
+    if (i < D.m) dzc = update_position(D, u, i);
+    if (u.phase == 2 && u.nflips > 0) {
         dzc = block_sum<BS>(dzc);
         if (threadIdx.x == 0) D.red[blockIdx.x] = dzc;
     }
     if (!last_block(&c->tickets[7])) return;
     __shared__ double g[1024];
-    if (threadIdx.x == 0) {
-        const int p = c->p, q = c->q, q_idx = c->q_idx;
-        if (!D.dense) D.beta[p_idx] = bp / (ap * ap);
-        if (phase == 2) {
-            double dz = c->dz;
-            if (nflips > 0) for (int b = 0; b < (int)gridDim.x; ++b) dz -= __ldcg(&D.red[b]);
-            c->obj += dz;
-            D.x[q] = D.x[q] + theta_P;
-        } else {
-            D.f[p_idx] = D.f[p_idx] / ap + c->dz;   // + infisibilityCorr
-        }
-        D.basis[p_idx] = q;
-        D.nonbasis[q_idx] = p;
-        D.var_pos[q] = p_idx;
-        D.var_pos[p] = -(q_idx + 1);
-        if (D.enter_count) { D.enter_count[q] += 1; D.entered_at[q] = c->iteration; }
-        if (phase == 2 && nflips > 0) {
-            for (int u = 0; u < D.n; ++u) {
-                const int code = D.flip_list[u];
-                if (u >= nflips) break;
-                if (code >= 0) D.x[code] = D.ub[code];
-                else D.x[-code - 1] = D.lb[-code - 1];
-            }
-        }
-        const double theta = c->theta;
-        if (phase == 2) {
-            c->obj += theta * c->delta_bfrt;
-            if (fabs(theta) < EPS_A) c->cycle += 1;
-        } else {
-            c->cycle = (fabs(theta) < EPS_A) ? c->cycle + 1 : 0;
-        }
-        if (!D.dense) D.eta_pos[T] = p_idx;
-        c->pivots += 1;
-        if (phase == 2 && c->trace_n < c->trace_cap) {
-            const int tn = c->trace_n;
-            D.trace[2 * tn] = p; D.trace[2 * tn + 1] = q;
-            D.trace_d[2 * tn] = theta; D.trace_d[2 * tn + 1] = c->obj;
-        }
-        if (phase == 2) c->trace_n += 1;
-    }
+    if (threadIdx.x == 0) update_tail(D, c, u, (int)gridDim.x);
     if (D.dense) return;   // no eta file in dense mode
+    const int T = u.T, p_idx = u.p_idx;
     // new row of G: G[T][u] = eta_u[p_T] - [p_u == p_T]
-    for (int u = threadIdx.x; u < T; u += BS)
-        g[u] = D.eta[(size_t)u * D.m + p_idx] - (D.eta_pos[u] == p_idx ? 1.0 : 0.0);
+    for (int v = threadIdx.x; v < T; v += BS)
+        g[v] = D.eta[(size_t)v * D.m + p_idx] - (D.eta_pos[v] == p_idx ? 1.0 : 0.0);
     __syncthreads();
-    for (int u = threadIdx.x; u < T; u += BS) D.Mtri[(size_t)T * D.cap + u] = g[u];
+    for (int v = threadIdx.x; v < T; v += BS) D.Mtri[(size_t)T * D.cap + v] = g[v];
     __syncthreads();
     if (threadIdx.x == 0) {
         c->T = T + 1;
@@ -1469,29 +1498,31 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
         case S_BINV: return launch_binv_update(D, 0, s);
         case S_SCORE: return launch_score(D, s);
         case S_CHUZR:
-            if (D.dense) k_chuzr_cta<1024><<<1, 1024, 0, s>>>(D);
-            else k_chuzr<BS><<<nblk(D.m > D.n ? D.m : D.n), BS, g_smem_bytes(D.cap), s>>>(D);
+            if (D.dense) { cudaError_t e = launch_pdl(k_chuzr_cta<1024>, dim3(1), dim3(1024), 0, s, D); if (e) return e; }
+            else { cudaError_t e = launch_pdl(k_chuzr<BS>, dim3(nblk(D.m > D.n ? D.m : D.n)), dim3(BS), g_smem_bytes(D.cap), s, D); if (e) return e; }
             break;
-        case S_BTRAN_RHS: if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, 0); else return cudaSuccess; break;
+        case S_BTRAN_RHS: { cudaError_t e = launch_pdl(k_btran_rhs<BS>, dim3(nblk(D.k)), dim3(BS), 0, s, D, 0); if (e) return e; break; }
         case S_BTRAN_GEMV: {
             const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
-            k_btran_gemv<BS><<<nbw + nblk(D.m), BS, 0, s>>>(D, D.rho, 0);
+            cudaError_t e = launch_pdl(k_btran_gemv<BS>, dim3(nbw + nblk(D.m)), dim3(BS), 0, s, D, D.rho, 0);
+            if (e) return e;
             break;
         }
-        case S_PIVOT_ROW: k_pivot_row<BS><<<nblk(D.n), BS, 0, s>>>(D, 3); break;
-        case S_DUAL_UPDATE: k_dual_update<BS><<<nblk(D.dense && D.m > D.n ? D.m : D.n), BS, 0, s>>>(D); break;
+        case S_PIVOT_ROW: { cudaError_t e = launch_pdl(k_pivot_row<BS>, dim3(nblk(D.n)), dim3(BS), 0, s, D, 3); if (e) return e; break; }
+        case S_DUAL_UPDATE: { cudaError_t e = launch_pdl(k_dual_update<BS>, dim3(nblk(D.dense && D.m > D.n ? D.m : D.n)), dim3(BS), 0, s, D); if (e) return e; break; }
         case S_FTRAN_K:
             if (D.k > 0) {
                 dim3 g(D.ftr_ntile, D.ftr_nchunk);
                 const size_t sh = (size_t)D.ftr_chunk * MAX_FTRAN_RHS * sizeof(double);
-                k_ftran_k2<BS><<<g, BS, sh, s>>>(D, 0, 0);
+                cudaError_t e = launch_pdl(k_ftran_k2<BS>, g, dim3(BS), sh, s, D, 0, 0);
+                if (e) return e;
             } else {
                 return cudaSuccess;
             }
             break;
-        case S_FTRAN_ASM: k_ftran_assemble<BS><<<nblk(D.m), BS, g_smem_bytes(D.cap), s>>>(D, 0, 0); break;
-        case S_ETA_APPLY: k_eta_apply<BS_ETA><<<(D.m + BS_ETA - 1) / BS_ETA, BS_ETA, 0, s>>>(D, 0, 1, 0); break;
-        case S_UPDATE: k_update<BS><<<nblk(D.m), BS, 0, s>>>(D, 0); break;
+        case S_FTRAN_ASM: { cudaError_t e = launch_pdl(k_ftran_assemble<BS>, dim3(nblk(D.m)), dim3(BS), g_smem_bytes(D.cap), s, D, 0, 0); if (e) return e; break; }
+        case S_ETA_APPLY: { cudaError_t e = launch_pdl(k_eta_apply<BS_ETA>, dim3((D.m + BS_ETA - 1) / BS_ETA), dim3(BS_ETA), 0, s, D, 0, 1, 0); if (e) return e; break; }
+        case S_UPDATE: { cudaError_t e = launch_pdl(k_update<BS>, dim3(nblk(D.m)), dim3(BS), 0, s, D, 0); if (e) return e; break; }
         default: return cudaErrorInvalidValue;
     }
     count_launch(1);
@@ -1700,9 +1731,11 @@ __global__ void k_ftran_dense(Dev D, int check, int force) {
 // B^-1 <- E B^-1 with E the eta of (alpha_q, p): row p scaled by 1/alpha_p, row i
 // minus alpha_q[i]/alpha_p times row p; fused with the exact DSE weights
 // beta_i = ||row i of B^-1||^2 (chunk partials, summed in chunk order by the
-// last block of each column tile).  Grid: (position tiles, row chunks).
+// last block of each column tile).  Grid: (position tiles, row chunks).  Runs
+// after k_update, whose bound-flip correction still needs the old B^-1.
 template <int BS>
 __global__ void k_binv_update(Dev D, int force) {
+    pdl_enter();
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
     const int p = c->p_idx;
@@ -1719,12 +1752,12 @@ __global__ void k_binv_update(Dev D, int force) {
         for (; r + 8 <= r1; r += 8) {
             double v[8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v[u] = col[(size_t)(r + u) * M];
+            for (int k = 0; k < 8; ++k) v[k] = col[(size_t)(r + k) * M];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const double piv = D.rho[r + u] * inv;
-                const double nv = isp ? piv : v[u] - f * piv;
-                col[(size_t)(r + u) * M] = nv;
+            for (int k = 0; k < 8; ++k) {
+                const double piv = D.rho[r + k] * inv;
+                const double nv = isp ? piv : v[k] - f * piv;
+                col[(size_t)(r + k) * M] = nv;
                 acc += nv * nv;
             }
         }
@@ -1807,7 +1840,8 @@ cudaError_t launch_ftran_dense(const Dev& D, int check, int force, cudaStream_t 
 }
 
 cudaError_t launch_binv_update(const Dev& D, int force, cudaStream_t s) {
-    k_binv_update<BS><<<dim3(nblk(D.m), D.binv_chunks), BS, 0, s>>>(D, force);
+    cudaError_t e = launch_pdl(k_binv_update<BS>, dim3(nblk(D.m), D.binv_chunks), dim3(BS), 0, s, D, force);
+    if (e != cudaSuccess) return e;
     count_launch(1);
     LAUNCH_OK();
     return cudaSuccess;

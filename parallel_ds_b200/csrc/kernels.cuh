@@ -33,6 +33,33 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s);
 bool score_step_active(const Dev& D);
 cudaError_t launch_score(const Dev& D, cudaStream_t s);
 
+// Programmatic dependent launch: the iteration kernels are launched with
+// programmatic stream serialisation, so a kernel's CTAs become resident while
+// its predecessor still runs and start the moment it completes (its memory
+// visible).  Each such kernel begins with pdl_enter(); launched without the
+// attribute, the two instructions do nothing.
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+#endif
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Kernel launch accounting (graph replays are added by the caller).
 void count_launch(int nk);
 void set_launch_counting(bool on);

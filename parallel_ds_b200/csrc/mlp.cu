@@ -211,6 +211,7 @@ constexpr uint32_t KB_A = 128 * 16 * 2;   // bytes of a 128-row, 16-wide K block
 constexpr uint32_t KB_B = 64 * 16 * 2;    // bytes of a 64-row, 16-wide K block
 
 __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
+    if (mode == 1) pdl_enter();
     __shared__ __align__(1024) unsigned char sA1[KB_A];          // X tile, 128 x 16
     __shared__ __align__(1024) unsigned char sB1[KB_B];          // W1, 64 x 16
     __shared__ __align__(1024) unsigned char sA2[4 * KB_A];      // H1 tile, 128 x 64
@@ -305,6 +306,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
 
 // Feature trace without a network (plain DSE solves that produce training data).
 __global__ void __launch_bounds__(128) k_features(Dev D) {
+    pdl_enter();
     const Ctl* c = D.ctl;
     if (*(volatile const int*)&c->halt || c->phase != 2) return;
     const int it = pricing_iteration(c);
@@ -594,9 +596,11 @@ cudaError_t launch_score(const Dev& D, cudaStream_t s) {
     if (D.learned) {
         FwdArgs a{nullptr, D.m, (const __nv_bfloat16*)D.mlp_w1, (const __nv_bfloat16*)D.mlp_w2, D.mlp_p,
                   nullptr, nullptr, nullptr, D.mlp_err};
-        k_mlp_fwd<<<grid, 128, 0, s>>>(a, D, 1);
+        cudaError_t e = launch_pdl(k_mlp_fwd, dim3(grid), dim3(128), 0, s, a, D, 1);
+        if (e != cudaSuccess) return e;
     } else if (D.ftr_every > 0) {
-        k_features<<<grid, 128, 0, s>>>(D);
+        cudaError_t e = launch_pdl(k_features, dim3(grid), dim3(128), 0, s, D);
+        if (e != cudaSuccess) return e;
     } else {
         return cudaSuccess;
     }
