@@ -87,6 +87,9 @@ typedef struct ds_options {
     int    learned_start_iteration; /* learned pricing: iterations before this one use
                                   DSE while the PDHG warm start runs on a second
                                   stream (default -1 = m/8; 0 = wait for it first) */
+    int    pdhg_cluster;       /* 1: run the PDHG warm start inside one 16-CTA thread-
+                                  block cluster when the LP fits its shared memory
+                                  (default 1); 0: always the launch-per-step graph */
 } ds_options;
 
 typedef struct ds_stats {

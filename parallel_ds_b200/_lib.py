@@ -25,7 +25,8 @@ class DsOptions(C.Structure):
                 ("strict_reference", C.c_int), ("seed", C.c_ulonglong), ("device", C.c_int),
                 ("stream", C.c_void_p), ("learned_margin", C.c_double), ("verbose", C.c_int),
                 ("learned_mix", C.c_double), ("learned_pdhg_iters", C.c_int), ("dense_max_m", C.c_int),
-                ("dense_refactor_interval", C.c_int), ("learned_start_iteration", C.c_int)]
+                ("dense_refactor_interval", C.c_int), ("learned_start_iteration", C.c_int),
+                ("pdhg_cluster", C.c_int)]
 
 
 class DsStats(C.Structure):

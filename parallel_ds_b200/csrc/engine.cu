@@ -130,6 +130,7 @@ struct Engine {
     DBuf<unsigned> d_binv_tickets;
     static constexpr int BINV_RC = 32;    // rows of B^-1 per chunk of the tiled kernels
     PdhgDev PD{};
+    PdhgClusterGeom pd_geom{0, 0, 0, 0, 0, 0};
     cudaGraphExec_t pd_gexec = nullptr;
     static constexpr int PDHG_RESTART = 500;
     cudaEvent_t evp0 = nullptr, evp1 = nullptr;
@@ -324,6 +325,8 @@ struct Engine {
         d_pd_x.ensure(stream, n); d_pd_xbar.ensure(stream, n); d_pd_xsum.ensure(stream, n); d_pd_y.ensure(stream, m); d_pd_ysum.ensure(stream, m);
         d_pd_gap.ensure(stream, N); d_pd_dual.ensure(stream, N);
         if (pd_gexec) { cudaGraphExecDestroy(pd_gexec); pd_gexec = nullptr; }
+        pd_geom = opt.pdhg_cluster ? pdhg_cluster_geometry(m, n, h_cptr.data(), h_rptr.data())
+                                   : PdhgClusterGeom{0, 0, 0, 0, 0, 0};
     }
 
     // ceil(iters / PDHG_RESTART) restart periods of PDHG from the zero start,
@@ -346,9 +349,11 @@ struct Engine {
             cudaGraphDestroy(g);
         }
         const int periods = (iters + PDHG_RESTART - 1) / PDHG_RESTART;
-        for (int p = 0; p < periods; ++p) CK(cudaGraphLaunch(pd_gexec, ps));
-        count_launch(periods * 2 * PDHG_RESTART);
-        CK(launch_pdhg_finish(PD, ps));
+        if (!launch_pdhg_cluster(PD, pd_geom, periods, ps)) {   // fallback: graph of 1000 launches per period
+            for (int p = 0; p < periods; ++p) CK(cudaGraphLaunch(pd_gexec, ps));
+            count_launch(periods * 2 * PDHG_RESTART);
+            CK(launch_pdhg_finish(PD, ps));
+        }
         CK(launch_pdhg_evidence(PD, d_pd_gap.p, d_pd_dual.p, ps));
     }
 
@@ -1182,6 +1187,7 @@ struct Engine {
         st.iterations = hc->iteration;
         st.learned_used = hc->learned_used;
         st.learned_fallback = hc->learned_fallback;
+        st.bfrt_flips = hc->flips_total;
         if (ftr_every > 0) fetch_feature_trace();
         model_wait_timeout = false;
         if (D.learned && D.mlp_err) {
@@ -1245,6 +1251,7 @@ void ds_default_options(ds_options* o) {
     o->dense_max_m = 4096;
     o->dense_refactor_interval = 400;
     o->learned_start_iteration = -1;
+    o->pdhg_cluster = 1;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }

@@ -80,6 +80,7 @@ struct Ctl {
     int window_fallbacks;       // CHUZC tie-window scans that needed the full scan
     int ftr_n;                  // feature-trace records written (may exceed the capacity)
     int ninfeas;                // primal infeasible positions at the last pricing
+    int flips_total;            // bound flips of the BFRT ratio test, whole solve
     int err;
     unsigned tickets[TICKETS];
 };

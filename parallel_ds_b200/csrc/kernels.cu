@@ -1151,6 +1151,7 @@ __device__ void update_tail(const Dev& D, Ctl* c, const UpdArgs& u, int nred) {
     D.var_pos[p] = -(q_idx + 1);
     if (D.enter_count) { D.enter_count[q] += 1; D.entered_at[q] = c->iteration; }
     if (u.phase == 2 && u.nflips > 0) {
+        c->flips_total += u.nflips;
         for (int k = 0; k < D.n; ++k) {
             const int code = D.flip_list[k];
             if (k >= u.nflips) break;

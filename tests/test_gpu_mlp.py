@@ -202,3 +202,18 @@ def test_trained_scorer_gain_on_held_out_lps(seed):
     assert st0["iterations"] >= 2.0 * st1["iterations"], (st0["iterations"], st1["iterations"])
     assert st1["learned_used"] > 0.8 * (st1["learned_used"] + st1["learned_fallback"])
     assert st1["pdhg_ms"] > 0.0
+
+
+@pytest.mark.parametrize("which", ["small", "learned"])
+def test_pdhg_cluster_matches_graph_path(which):
+    """The one-cluster PDHG (shared-memory slices, DSMEM replicas, cluster
+    barriers) against the launch-per-step graph path on the same LP:
+    |x_cluster - x_graph| <= 1e-9 (1 + |x_graph|) (summation orders differ)."""
+    lp = L.plain_small(seed=6) if which == "small" else L.learned(seed=3)
+    res = []
+    for cl in (1, 0):
+        s = S.CudaDualSimplex(S.problem_from_lp(lp), pdhg_cluster=cl)
+        s.initDualSimplex()
+        res.append(s.pdhg_estimate(1000))
+    (xc, yc), (xg, yg) = res
+    assert close(xc, xg, 1e-9) and close(yc, yg, 1e-9)

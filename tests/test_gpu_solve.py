@@ -139,9 +139,13 @@ def test_load_csr_general_bounds():
     m, n = lp["m"], lp["n"]
     col_lb = np.zeros(n); col_ub = np.where(rng.random(n) < 0.3, 0.5, 1e300)
     row_lb = np.where(rng.random(m) < 0.2, lp["b"] - 50.0, -1e300); row_ub = lp["b"].copy()
+    from parallel_ds_b200._lib import DsOptions, DsStats
     L_ = lib()
+    o = DsOptions()
+    L_.ds_default_options(C.byref(o))
+    o.dense_max_m = MODE["dense_max_m"]
     h = C.c_void_p()
-    assert L_.ds_create(None, C.byref(h)) == 0
+    assert L_.ds_create(C.byref(o), C.byref(h)) == 0
     try:
         rc = L_.ds_load_csr(h, m, n, ptr(lp["row_ptr"], C.c_int), ptr(lp["col_idx"], C.c_int),
                             ptr(lp["val"], C.c_double), ptr(lp["c"], C.c_double), ptr(col_lb, C.c_double),
@@ -150,6 +154,9 @@ def test_load_csr_general_bounds():
         assert L_.ds_solve(h) == 0
         assert L_.ds_get_status(h) == 1
         z = L_.ds_get_objective(h)
+        st = DsStats()
+        L_.ds_get_stats(h, C.byref(st))
+        assert st.bfrt_flips > 0                  # the bound-flipping ratio test was exercised
     finally:
         L_.ds_destroy(h)
     from scipy.optimize import linprog
