@@ -521,6 +521,13 @@ def solve_one(args):
     from parallel_ds_b200 import lp as L
     from parallel_ds_b200 import solver as S
     lp = gen(args.workload, args.solve_one)
+    if args.pdhg_estimate:
+        s = S.CudaDualSimplex(S.problem_from_lp(lp), pdhg_cluster=0 if args.no_pdhg_cluster else 1)
+        s.initDualSimplex()
+        x, y = s.pdhg_estimate(args.pdhg_estimate)
+        print(json.dumps({"workload": args.workload, "seed": args.solve_one, "pdhg_iterations": args.pdhg_estimate,
+                          "objective_estimate": float(np.dot(lp["c"], x))}))
+        return
     model = LN.LeavingRowScorer.load(args.weights) if args.pricing == "learned" else None
     out = []
     for rep in range(args.repeat):
@@ -530,7 +537,6 @@ def solve_one(args):
         sol = s.solve()
         out.append(dict(status=s.status(), objective=sol.Z, **{k: v for k, v in s.stats().items()}))
     print(json.dumps({"workload": args.workload, "seed": args.solve_one, "pricing": args.pricing, "solves": out}))
-    del np
 
 
 def main():
@@ -549,6 +555,9 @@ def main():
     ap.add_argument("--solve-one", type=int, default=None, metavar="SEED",
                     help="solve one LP of the workload alone and print its stats (profiling)")
     ap.add_argument("--repeat", type=int, default=1, help="--solve-one: solves of the same LP")
+    ap.add_argument("--pdhg-estimate", type=int, default=0, metavar="ITERS",
+                    help="--solve-one: run only the PDHG warm-start estimate for ITERS iterations")
+    ap.add_argument("--no-pdhg-cluster", action="store_true", help="PDHG on the launch-per-step graph path")
     ap.add_argument("--no-tune", action="store_true", help="batched workloads: default schedule, no autotuning")
     ap.add_argument("--max-iterations", type=int, default=0, help="--solve-one: iteration cap (0: none)")
     ap.add_argument("--batch-count", type=int, default=0,
