@@ -98,3 +98,25 @@ def test_basis_solve_rhs_counts(learned_bases, nr):
     ref = np.linalg.solve(B, rhs)
     got = gpu_solve(lp, basis, rhs, 0)
     assert np.abs(got - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("k", [1601, 2400])
+def test_basis_solve_bump_above_shared_memory_panel(k):
+    """A structural bump larger than the shared-memory panel limit (1600 rows),
+    so the Gauss-Jordan panels run from global memory: random structural columns
+    of a sparse 1%-dense LP plus slacks for the other rows, checked against a
+    dense solve."""
+    m = k + 600
+    lp = L.generate(m=m, n=2 * m, density=0.01, seed=k)
+    r = np.random.default_rng(k)
+    cols = np.sort(r.choice(lp["n"], size=k, replace=False))
+    slack_rows = np.sort(r.choice(m, size=m - k, replace=False))
+    basis = np.concatenate([cols, lp["n"] + slack_rows]).astype(np.int32)
+    r.shuffle(basis)
+    B = dense_basis(lp, basis)
+    assert np.linalg.matrix_rank(B) == m            # a nonsingular basis
+    rhs = r.normal(size=m)
+    for transpose in (0, 1):
+        x = gpu_solve(lp, basis, rhs, transpose)
+        ref = np.linalg.solve(B.T if transpose else B, rhs)
+        assert np.max(np.abs(x - ref)) <= 1e-9 * (1 + np.max(np.abs(ref))), transpose
