@@ -240,22 +240,62 @@ __device__ void solve_instance(const BatchDev& B, const Group& G, int inst, unsi
             // weights.  Thread i owns row i and walks the columns; eight independent
             // loads per step keep enough bytes in flight to stream B^-1 from L2/HBM.
             const double inv = 1.0 / app;
-            for (int i = t; i < m; i += g) {
-                const double f = aq[i];
-                const bool isp = (i == p);
+            if (m <= g) {
+                // one row per thread
+                for (int i = t; i < m; i += g) {
+                    const double f = aq[i];
+                    const bool isp = (i == p);
+                    double* col = Binv + i;
+                    double acc = 0.0;
+                    int k = 0;
+                    for (; k + 8 <= m; k += 8) {
+                        double v[8];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) v[u] = col[(long long)(k + u) * m];
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const double piv = rho[k + u] * inv;
+                            const double nv = isp ? piv : v[u] - f * piv;
+                            col[(long long)(k + u) * m] = nv;
+                            acc += nv * nv;
+                        }
+                    }
+                    for (; k < m; ++k) {
+                        const double piv = rho[k] * inv;
+                        const double nv = isp ? piv : col[(long long)k * m] - f * piv;
+                        col[(long long)k * m] = nv;
+                        acc += nv * nv;
+                    }
+                    beta[i] = acc;
+                }
+            } else
+            // two rows per pass (i and i + g): sixteen independent loads in flight
+            for (int i = t; i < m; i += 2 * g) {
+                const int i2 = i + g;
+                const bool two = i2 < m;
+                const double f = aq[i], f2 = two ? aq[i2] : 0.0;
+                const bool isp = (i == p), isp2 = (i2 == p);
                 double* col = Binv + i;
-                double acc = 0.0;
+                double acc = 0.0, acc2 = 0.0;
                 int k = 0;
                 for (; k + 8 <= m; k += 8) {
-                    double v[8];
+                    double v[8], w[8];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) v[u] = col[(long long)(k + u) * m];
+                    for (int u = 0; u < 8; ++u) {
+                        v[u] = col[(long long)(k + u) * m];
+                        w[u] = two ? col[(long long)(k + u) * m + g] : 0.0;
+                    }
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const double piv = rho[k + u] * inv;
                         const double nv = isp ? piv : v[u] - f * piv;
                         col[(long long)(k + u) * m] = nv;
                         acc += nv * nv;
+                        if (two) {
+                            const double nw = isp2 ? piv : w[u] - f2 * piv;
+                            col[(long long)(k + u) * m + g] = nw;
+                            acc2 += nw * nw;
+                        }
                     }
                 }
                 for (; k < m; ++k) {
@@ -263,8 +303,14 @@ __device__ void solve_instance(const BatchDev& B, const Group& G, int inst, unsi
                     const double nv = isp ? piv : col[(long long)k * m] - f * piv;
                     col[(long long)k * m] = nv;
                     acc += nv * nv;
+                    if (two) {
+                        const double nw = isp2 ? piv : col[(long long)k * m + g] - f2 * piv;
+                        col[(long long)k * m + g] = nw;
+                        acc2 += nw * nw;
+                    }
                 }
                 beta[i] = acc;
+                if (two) beta[i2] = acc2;
             }
             gsync(G);
             if (t == 0) {
