@@ -856,16 +856,19 @@ __global__ void k_dual_update(Dev D) {
         if (phase == 1) c->z_phase1 = c->z_phase1 - theta * c->f_p;
     }
     __syncthreads();
-    // entering column a_q as a dense row vector (clear the previous one first)
-    const int pq = c->prev_q;
+    // entering column a_q as a dense row vector (clear the previous one first);
+    // the eta-file FTRAN reads it, dense mode does not
+    const int pq = D.dense ? -1 : c->prev_q;
     if (pq >= 0) {
         if (pq < D.n) { for (int e = D.cptr[pq] + threadIdx.x; e < D.cptr[pq + 1]; e += BS) D.aq_dense[D.crow[e]] = 0.0; }
         else if (threadIdx.x == 0) D.aq_dense[pq - D.n] = 0.0;
     }
     __syncthreads();
     const int q = c->q;
-    if (q < D.n) { for (int e = D.cptr[q] + threadIdx.x; e < D.cptr[q + 1]; e += BS) D.aq_dense[D.crow[e]] = D.cval[e]; }
-    else if (threadIdx.x == 0) D.aq_dense[q - D.n] = 1.0;
+    if (!D.dense) {
+        if (q < D.n) { for (int e = D.cptr[q] + threadIdx.x; e < D.cptr[q + 1]; e += BS) D.aq_dense[D.crow[e]] = D.cval[e]; }
+        else if (threadIdx.x == 0) D.aq_dense[q - D.n] = 1.0;
+    }
     if (threadIdx.x == 0) { c->prev_q = q; c->nrhs = (s_nf > 0) ? 3 : 2; }
     if (s_nf == 0) { if (threadIdx.x == 0) c->dz = (phase == 2) ? 0.0 : c->dz; return; }
     // ---- flips (rare): ordered lists, column change and delta_z in slot order
