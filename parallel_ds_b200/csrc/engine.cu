@@ -47,6 +47,10 @@ constexpr double INF_OBJ = 1e25;
 // iteration and the batch's remaining launches return at once (a few
 // microseconds each), so long batches cost little and save host round trips.
 constexpr int BATCH_ITERS = 100;
+// Iterations per launch of the unrolled iteration graph: inside one graph the
+// kernels of consecutive iterations are chained by programmatic dependencies,
+// so the boundary between iterations costs no graph launch.
+constexpr int GRAPH_UNROLL = 8;
 
 // Blocks freed to the device's default memory pool stay cached for reuse
 // (release threshold: unlimited) instead of going back to the driver at each
@@ -146,7 +150,8 @@ struct Engine {
 
     Ctl* hc = nullptr;          // pinned host mirror of Ctl
     Dev D{};
-    cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec = nullptr;     // one iteration
+    cudaGraphExec_t gexec_u = nullptr;   // GRAPH_UNROLL iterations
     int cap = 0;
     int k = 0;
 
@@ -192,6 +197,7 @@ struct Engine {
     }
     ~Engine() {
         if (gexec) cudaGraphExecDestroy(gexec);
+        if (gexec_u) cudaGraphExecDestroy(gexec_u);
         if (hc) cudaFreeHost(hc);
         if (ev0) cudaEventDestroy(ev0);
         if (evp0) cudaEventDestroy(evp0);
@@ -281,8 +287,10 @@ struct Engine {
             const int chunks = (m + BINV_RC - 1) / BINV_RC;
             d_Binv.ensure(stream, (size_t)m * m);
             d_binv_part.ensure(stream, (size_t)chunks * m);
-            d_binv_tickets.ensure(stream, (size_t)(m + 255) / 256 + 1);
-            CK(cudaMemsetAsync(d_binv_tickets.p, 0, sizeof(unsigned) * ((m + 255) / 256 + 1), stream));
+            // one ticket per 32-position slice (k_binv_update) covers the
+            // 256-position tiles of k_dense_colsum too
+            d_binv_tickets.ensure(stream, (size_t)(m + 31) / 32 + 1);
+            CK(cudaMemsetAsync(d_binv_tickets.p, 0, sizeof(unsigned) * ((m + 31) / 32 + 1), stream));
         }
         std::vector<int> rc(m);
         for (int i = 0; i < m; ++i) rc[i] = h_rptr[i + 1] - h_rptr[i];
@@ -531,21 +539,30 @@ struct Engine {
 
     void invalidate_graph() {
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+        if (gexec_u) { cudaGraphExecDestroy(gexec_u); gexec_u = nullptr; }
     }
-    void ensure_graph() {
-        if (gexec) return;
+    // Capture `iters` consecutive iterations into one executable graph.
+    cudaGraphExec_t capture_iterations(int iters, long long* nodes) {
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         set_launch_counting(false);
-        cudaError_t le = launch_iteration(D, stream);
+        cudaError_t le = cudaSuccess;
+        for (int u = 0; u < iters && le == cudaSuccess; ++u) le = launch_iteration(D, stream);
         set_launch_counting(true);
         cudaError_t ce = cudaStreamEndCapture(stream, &g);
         CK(le); CK(ce);
         size_t nn = 0;
         CK(cudaGraphGetNodes(g, nullptr, &nn));
-        graph_nodes = (long long)nn;
-        CK(cudaGraphInstantiate(&gexec, g, 0));
+        if (nodes) *nodes = (long long)nn;
+        cudaGraphExec_t ge = nullptr;
+        CK(cudaGraphInstantiate(&ge, g, 0));
         cudaGraphDestroy(g);
+        return ge;
+    }
+    void ensure_graph() {
+        if (gexec) return;
+        gexec = capture_iterations(1, &graph_nodes);
+        gexec_u = capture_iterations(GRAPH_UNROLL, nullptr);
     }
 
     // -------------------------------------------------------------- solves
@@ -770,7 +787,7 @@ struct Engine {
             case S_ETA_APPLY: return 8 * Tt * M + 16 * R * M;
             case S_UPDATE: return dense ? 44 * M : 60 * M + 8 * Tt + 4 * Tt * Tt;
             case S_FTRAN_DENSE: return (12.0 + 8 * M) * ((double)h_rptr[m] / n) + 8 * M;
-            case S_BINV: return 16 * M * M + 16 * M + 8 * M * ((M + BINV_RC - 1) / BINV_RC);
+            case S_BINV: return 16 * M * M + 16 * M + 8 * M * ((M + BINV_ROWS - 1) / BINV_ROWS);
         }
         return 0;
     }
@@ -902,7 +919,9 @@ struct Engine {
             if (batch > BATCH_ITERS) batch = BATCH_ITERS;
             if (batch < 1) batch = 1;
             pd_wait_before(it + batch);
-            for (int b = 0; b < batch; ++b) CK(cudaGraphLaunch(gexec, stream));
+            int b = 0;
+            for (; b + GRAPH_UNROLL <= batch; b += GRAPH_UNROLL) CK(cudaGraphLaunch(gexec_u, stream));
+            for (; b < batch; ++b) CK(cudaGraphLaunch(gexec, stream));
             count_launch((int)(batch * graph_nodes));
             pull();
             if (hc->halt) return hc->event;

@@ -682,24 +682,32 @@ __global__ void k_pivot_row(Dev D, int mode) {
     Min2 mm{CUDART_INF, INT_MAX, CUDART_INF};
     if (i < D.n) {
         const int j = D.nonbasis[i];
+        // the candidate test's operands depend only on j: load them with the dot's
+        unsigned char tj = 0;
+        double dj = 0.0, xj = 0.0, lj = 0.0, uj = 0.0;
+        if (mode & 2) { dj = D.d[j]; tj = D.type[j]; xj = D.x[j]; lj = D.lb[j]; uj = D.ub[j]; }
         double acc = 0.0;
         if (mode & 1) {
             if (j < D.n) {
                 // the CSC order of the reference's dot (matrix.cpp:273-286), with the
-                // loads of eight nonzeros issued before their products are summed
+                // loads of sixteen nonzeros (the last batch predicated) issued before
+                // their products are summed
                 const int e1 = D.cptr[j + 1];
-                int e = D.cptr[j];
-                for (; e + 8 <= e1; e += 8) {
-                    int rr[8];
-                    double vv[8], pp[8];
+                for (int e = D.cptr[j]; e < e1; e += 16) {
+                    int rr[16];
+                    double vv[16], pp[16];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) { rr[u] = D.crow[e + u]; vv[u] = D.cval[e + u]; }
+                    for (int u = 0; u < 16; ++u) {
+                        const bool ok = e + u < e1;
+                        rr[u] = ok ? D.crow[e + u] : 0;
+                        vv[u] = ok ? D.cval[e + u] : 0.0;
+                    }
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) pp[u] = D.rho[rr[u]];
+                    for (int u = 0; u < 16; ++u) pp[u] = D.rho[rr[u]];
 #pragma unroll
-                    for (int u = 0; u < 8; ++u) acc += vv[u] * pp[u];
+                    for (int u = 0; u < 16; ++u)
+                        if (e + u < e1) acc += vv[u] * pp[u];
                 }
-                for (; e < e1; ++e) acc += D.cval[e] * D.rho[D.crow[e]];
             } else {
                 acc += 1.0 * D.rho[j - D.n];
             }
@@ -709,9 +717,8 @@ __global__ void k_pivot_row(Dev D, int mode) {
         }
         if (mode & 2) {
             const double a = sgn_a * acc;
-            const double dj = D.d[j];
             bool cand;
-            if (phase == 2) cand = rt_candidate(a, D.type[j], D.x[j], D.lb[j], D.ub[j]);
+            if (phase == 2) cand = rt_candidate(a, tj, xj, lj, uj);
             else cand = (dj >= 0 && a > EPS_A) || (dj <= 0 && a < -EPS_A);
             double th = CUDART_NAN;
             if (cand) {
@@ -821,18 +828,40 @@ __global__ void k_dual_update(Dev D) {
         D.flip[i] = fl;
         nf = fl ? 1 : 0;
     }
-    if (D.dense && i < D.m) {
-        // dense mode: the iteration FTRAN alpha_q = B^-1 a_q rides on this grid
+    if (D.dense && blockIdx.x * BS < D.m) {   // block-uniform
+        // dense mode: the iteration FTRAN alpha_q = B^-1 a_q rides on this grid.
+        // The entering column's nonzeros are staged in shared memory, so that
+        // every thread issues sixteen B^-1 loads before summing them in order.
+        __shared__ int s_r[BS + 16];   // rows past the column's end read row 0 (not summed)
+        __shared__ double s_v[BS];
         const int q = c->q;
         const size_t M = D.m;
         double sq = 0.0;
+        if (threadIdx.x < 16) s_r[BS + threadIdx.x] = 0;
         if (q < D.n) {
-#pragma unroll 4
-            for (int e = D.cptr[q]; e < D.cptr[q + 1]; ++e) sq += D.Binv[(size_t)D.crow[e] * M + i] * D.cval[e];
-        } else {
+            const int e0 = D.cptr[q], e1 = D.cptr[q + 1];
+            for (int eb = e0; eb < e1; eb += BS) {
+                const int cnt = min(BS, e1 - eb);
+                __syncthreads();
+                const bool in = (int)threadIdx.x < cnt;
+                s_r[threadIdx.x] = in ? D.crow[eb + threadIdx.x] : 0;
+                if (in) s_v[threadIdx.x] = D.cval[eb + threadIdx.x];
+                __syncthreads();
+                if (i < D.m) {
+                    for (int u0 = 0; u0 < cnt; u0 += 16) {
+                        double bv[16];
+#pragma unroll
+                        for (int u = 0; u < 16; ++u) bv[u] = D.Binv[(size_t)s_r[u0 + u] * M + i];
+#pragma unroll
+                        for (int u = 0; u < 16; ++u)
+                            if (u0 + u < cnt) sq += bv[u] * s_v[u0 + u];
+                    }
+                }
+            }
+        } else if (i < D.m) {
             sq = D.Binv[(size_t)(q - D.n) * M + i];
         }
-        D.alpha_q[i] = sq;
+        if (i < D.m) D.alpha_q[i] = sq;
     }
     nf = block_sum_int<BS>(nf);
     if (threadIdx.x == 0) D.redi[blockIdx.x] = nf;
@@ -1737,21 +1766,44 @@ __global__ void k_ftran_dense(Dev D, int check, int force) {
 // beta_i = ||row i of B^-1||^2 (chunk partials, summed in chunk order by the
 // last block of each column tile).  Grid: (position tiles, row chunks).  Runs
 // after k_update, whose bound-flip correction still needs the old B^-1.
+// Sum of the chunk partials part[y * M + i], y = 0..ny-1, in chunk order, with
+// sixteen loads in flight per batch.
+__device__ __forceinline__ double sum_chunk_parts(const double* part, size_t M, int i, int ny) {
+    double b = 0.0;
+    for (int y0 = 0; y0 < ny; y0 += 16) {
+        double t[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) t[k] = (y0 + k < ny) ? __ldcg(&part[(size_t)(y0 + k) * M + i]) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            if (y0 + k < ny) b += t[k];
+    }
+    return b;
+}
+
+// B^-1 <- E B^-1 for the pivot (p, alpha_q) (Binv[r * m + i] = (B^-1)_{i,r}),
+// with beta_i = ||row i of B^-1||^2 summed from the updated values.  A block
+// covers 32 positions i (a lane each: one coalesced 256-byte segment per row)
+// and BINV_ROWS rows r, BINV_RW per warp; the warps' sums are added in warp
+// order in shared memory, and the last of a slice's row-chunk blocks adds the
+// chunk partials in chunk order (8 for m = 2000), so beta is deterministic.
 template <int BS>
-__global__ void k_binv_update(Dev D, int force) {
+__global__ void __launch_bounds__(BS) k_binv_update(Dev D, int force) {
+    static_assert(BS == 8 * 32, "eight warps per block");
     pdl_enter();
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
     const int p = c->p_idx;
     const size_t M = D.m;
     const double inv = 1.0 / __ldcg(&D.alpha_q[p]);
-    const int i = blockIdx.x * BS + threadIdx.x;
-    const int r0 = blockIdx.y * D.binv_rc, r1 = min(D.m, r0 + D.binv_rc);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane;
+    const int r0 = blockIdx.y * BINV_ROWS + warp * BINV_RW, r1 = min(D.m, r0 + BINV_RW);
+    double acc = 0.0;
     if (i < D.m) {
         const double f = D.alpha_q[i];
         const bool isp = (i == p);
         double* col = D.Binv + i;
-        double acc = 0.0;
         int r = r0;
         for (; r + 8 <= r1; r += 8) {
             double v[8];
@@ -1771,14 +1823,18 @@ __global__ void k_binv_update(Dev D, int force) {
             col[(size_t)r * M] = nv;
             acc += nv * nv;
         }
-        D.binv_part[(size_t)blockIdx.y * M + i] = acc;
+    }
+    __shared__ double s_acc[8][32];
+    s_acc[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0 && i < D.m) {
+        double b = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) b += s_acc[w][lane];
+        D.binv_part[(size_t)blockIdx.y * M + i] = b;
     }
     if (!last_in_tile(&D.binv_tickets[blockIdx.x])) return;
-    if (i < D.m) {
-        double b = 0.0;
-        for (int y = 0; y < (int)gridDim.y; ++y) b += __ldcg(&D.binv_part[(size_t)y * M + i]);
-        D.beta[i] = b;
-    }
+    if (warp == 0 && i < D.m) D.beta[i] = sum_chunk_parts(D.binv_part, M, i, (int)gridDim.y);
 }
 
 // y = B^-1 v (mode 0) or y_i = ||row i of B^-1||^2 (mode 1), same tiling.
@@ -1796,11 +1852,7 @@ __global__ void k_dense_colsum(Dev D, const double* v, double* y, int mode) {
         D.binv_part[(size_t)blockIdx.y * M + i] = acc;
     }
     if (!last_in_tile(&D.binv_tickets[blockIdx.x])) return;
-    if (i < D.m) {
-        double s = 0.0;
-        for (int yy = 0; yy < (int)gridDim.y; ++yy) s += __ldcg(&D.binv_part[(size_t)yy * M + i]);
-        y[i] = s;
-    }
+    if (i < D.m) y[i] = sum_chunk_parts(D.binv_part, M, i, (int)gridDim.y);
 }
 
 // y = B^-T c: one warp per constraint row r, a contiguous dot over positions.
@@ -1844,7 +1896,8 @@ cudaError_t launch_ftran_dense(const Dev& D, int check, int force, cudaStream_t 
 }
 
 cudaError_t launch_binv_update(const Dev& D, int force, cudaStream_t s) {
-    cudaError_t e = launch_pdl(k_binv_update<BS>, dim3(nblk(D.m), D.binv_chunks), dim3(BS), 0, s, D, force);
+    cudaError_t e = launch_pdl(k_binv_update<BS>, dim3((D.m + 31) / 32, (D.m + BINV_ROWS - 1) / BINV_ROWS), dim3(BS), 0, s,
+                               D, force);
     if (e != cudaSuccess) return e;
     count_launch(1);
     LAUNCH_OK();

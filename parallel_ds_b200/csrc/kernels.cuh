@@ -38,6 +38,10 @@ cudaError_t launch_score(const Dev& D, cudaStream_t s);
 // its predecessor still runs and start the moment it completes (its memory
 // visible).  Each such kernel begins with pdl_enter(); launched without the
 // attribute, the two instructions do nothing.
+// k_binv_update tiling: rows of B^-1 per warp and per 256-thread block.
+constexpr int BINV_RW = 32;
+constexpr int BINV_ROWS = 8 * BINV_RW;
+
 #ifdef __CUDACC__
 __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");

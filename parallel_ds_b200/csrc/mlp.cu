@@ -147,7 +147,11 @@ static_assert(NPARAMS == DS_MLP_NPARAMS, "parameter count");
 static_assert(NF <= 16, "features fit one K block");
 
 __device__ __forceinline__ float clampf(double v, double lo, double hi) { return (float)fmin(fmax(v, lo), hi); }
-__device__ __forceinline__ double lg10(double v) { return log10(fmax(v, 1e-300)); }
+// log10 of v clamped to [lo, hi] (lo >= -30), in single precision.
+__device__ __forceinline__ float lg10f(double v, float lo, float hi) {
+    const float a = (float)fmin(fmax(v, 1e-30), 1e30);
+    return fminf(fmaxf(log10f(a), lo), hi);
+}
 
 // Iteration number the pricing of this launch belongs to.
 __device__ __forceinline__ int pricing_iteration(const Ctl* c) { return c->iteration + (c->top_done ? 0 : 1); }
@@ -157,26 +161,36 @@ __device__ __forceinline__ int pricing_iteration(const Ctl* c) { return c->itera
 // primal infeasible, or a zero DSE weight), exactly the rows k_chuzr skips.
 __device__ bool row_features(const Dev& D, int i, int it, float* f) {
     const int j = D.basis[i];
-    const double x = D.x[j];
-    double dt = 0.0;
-    const bool inf = var_infeas(D.type[j], x, D.lb[j], D.ub[j], &dt) && fabs(dt) > 1e-8;
     const double be = D.beta[i];
-    const double w = inf ? (dt * dt) / be : 0.0;
-    const bool slack = j >= D.n;
+    const double x = D.x[j];
+    const unsigned char t = D.type[j];
+    const double l = D.lb[j], u = D.ub[j];
+    const float pg = D.pd_gap[j], pdu = D.pd_dual[j];
+    const int ec = D.enter_count[j], ea = D.entered_at[j];
     const Ctl* c = D.ctl;
-    const double wl = (c->beta_p > 0.0) ? (c->delta * c->delta) / c->beta_p : 0.0;   // last pick's weight
-    f[0] = slack ? 1.f : 0.f;
-    f[1] = clampf(lg10(fabs(dt)), -12, 4) / 4.f;
-    f[2] = clampf(lg10(be), -12, 12) / 4.f;
-    f[3] = clampf(lg10(w), -24, 12) / 4.f;
-    f[4] = (wl > 0.0 && w > 0.0) ? clampf(lg10(w / wl), -12, 12) / 4.f : 0.f;
-    f[5] = clampf(asinh(1000.0 * (double)D.pd_gap[j]) / 8.0, -2, 2);
-    f[6] = clampf(asinh(1000.0 * (double)D.pd_dual[j]) / 8.0, -2, 2);
-    f[7] = (float)c->ninfeas / (float)D.m;
+    const double bp = c->beta_p, dl = c->delta;
+    const int ninf = c->ninfeas;
+    double dt = 0.0;
+    const bool inf = var_infeas(t, x, l, u, &dt) && fabs(dt) > 1e-8;
+    const double w = inf ? (dt * dt) / be : 0.0;
+    const double wl = (bp > 0.0) ? (dl * dl) / bp : 0.0;   // last pick's weight
+    // The logarithms run in single precision (the features are rounded to
+    // bf16 for the tensor cores); arguments are floored at 1e-30, below every
+    // clamp, so that underflow to zero in the conversion changes nothing.
+    f[0] = (j >= D.n) ? 1.f : 0.f;
+    f[1] = lg10f(fabs(dt), -12.f, 4.f) * 0.25f;
+    f[2] = lg10f(be, -12.f, 12.f) * 0.25f;
+    f[3] = lg10f(w, -24.f, 12.f) * 0.25f;
+    f[4] = (wl > 0.0 && w > 0.0) ? lg10f(w / wl, -12.f, 12.f) * 0.25f : 0.f;
+    f[5] = fminf(fmaxf(asinhf(1000.f * pg) * 0.125f, -2.f), 2.f);
+    f[6] = fminf(fmaxf(asinhf(1000.f * pdu) * 0.125f, -2.f), 2.f);
+    f[7] = (float)ninf / (float)D.m;
     f[8] = clampf((double)it / D.m, 0, 10) / 5.f;
-    f[9] = (float)min(D.enter_count[j], 20) / 5.f;
-    f[10] = clampf((double)(it - D.entered_at[j]) / D.m, 0, 5);
-    f[11] = (float)copysign(log10(1.0 + fabs(x)), x);
+    f[9] = (float)min(ec, 20) / 5.f;
+    f[10] = clampf((double)(it - ea) / D.m, 0, 5);
+    const double ax = fabs(x);
+    const float lx = ax < 1e30 ? log10f(1.f + (float)ax) : (float)log10(1.0 + ax);
+    f[11] = x < 0.0 ? -lx : lx;
     for (int k = NF; k < 16; ++k) f[k] = 0.f;
     return inf && w > 0.0;
 }
@@ -211,7 +225,6 @@ constexpr uint32_t KB_A = 128 * 16 * 2;   // bytes of a 128-row, 16-wide K block
 constexpr uint32_t KB_B = 64 * 16 * 2;    // bytes of a 64-row, 16-wide K block
 
 __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
-    if (mode == 1) pdl_enter();
     __shared__ __align__(1024) unsigned char sA1[KB_A];          // X tile, 128 x 16
     __shared__ __align__(1024) unsigned char sB1[KB_B];          // W1, 64 x 16
     __shared__ __align__(1024) unsigned char sA2[4 * KB_A];      // H1 tile, 128 x 64
@@ -219,27 +232,38 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
     __shared__ uint64_t mbar;
     __shared__ uint32_t tmem_base;
     __shared__ int bad;
+    __shared__ float sP[3 * 64 + 1];                             // b1, b2, w3, b3
     const int tid = threadIdx.x, warp = tid >> 5;
     const int row = blockIdx.x * 128 + tid;
     const bool live = row < a.M;
-    int it = 0;
-    if (mode == 1) {
-        const Ctl* c = D.ctl;
-        if (*(volatile const int*)&c->halt || c->phase != 2) return;   // block-uniform
-        it = pricing_iteration(c);
-        if (it < D.learn_start) return;   // DSE prices these iterations; no scores needed
-    }
-    __shared__ float sP[3 * 64 + 1];                             // b1, b2, w3, b3
+    // Prologue that reads nothing the previous kernel writes (the weights are
+    // fixed during a solve): under programmatic dependent launch it overlaps
+    // the tail of that kernel.  The weights go straight into the K-major
+    // core-matrix layout with 16-byte loads.
+    if (mode == 1) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     if (tid == 0) { mbar_init(&mbar, 1); bad = 0; }
     if (warp == 0) tmem_alloc(&tmem_base, 128);
-    // weights first (independent of the features): 16-byte loads straight into
-    // the K-major core-matrix layout
     *reinterpret_cast<uint4*>(sB1 + kofs(tid >> 1, 8 * (tid & 1), KB_B)) = reinterpret_cast<const uint4*>(a.W1b)[tid];
 #pragma unroll
     for (int c = tid; c < 512; c += 128)
         *reinterpret_cast<uint4*>(sB2 + kofs(c >> 3, 8 * (c & 7), KB_B)) = reinterpret_cast<const uint4*>(a.W2b)[c];
     for (int e = tid; e < 3 * 64 + 1; e += 128)   // w3 and b3 are adjacent (OFF_W3 + 64 == OFF_B3)
         sP[e] = e < 64 ? a.P[OFF_B1 + e] : e < 128 ? a.P[OFF_B2 + e - 64] : a.P[OFF_W3 + e - 128];
+    int it = 0;
+    if (mode == 1) {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        const Ctl* c = D.ctl;
+        it = pricing_iteration(c);
+        // block-uniform: no scores when halted, in phase 1, or while DSE prices
+        // the first iterations; the TMEM columns are freed before returning
+        if (__ldcg(&c->halt) || c->phase != 2 || it < D.learn_start) {
+            tc_before_sync();
+            __syncthreads();
+            tc_after_sync();
+            if (warp == 0) tmem_dealloc(tmem_base, 128);
+            return;
+        }
+    }
     float f[16];
     bool cand = false;
     if (live) {
