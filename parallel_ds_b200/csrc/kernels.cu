@@ -31,12 +31,15 @@
 #include <climits>
 #include <cmath>
 
+#include <cooperative_groups.h>
 #include <math_constants.h>
 
 #include "engine.cuh"
 #include "kernels.cuh"
 
 namespace ds {
+
+namespace cg = cooperative_groups;
 
 __device__ __forceinline__ bool halted(const Ctl* c) { return *(volatile const int*)&c->halt != 0; }
 
@@ -357,8 +360,13 @@ __device__ __forceinline__ void chuzr_row(const Dev& D, int i, int phase, bool l
 // Thread 0's decision after the reductions of CHUZR: loop bookkeeping events,
 // the dual check, the optimality test, the leaving row (DSE or learned) or the
 // phase-1 outcome.  Returns the leaving position for the eta part of BTRAN, or -1.
+// What the decision needs of a winning row, recorded by the thread that scanned
+// it (cluster CHUZR), so that the deciding thread does not load it again.
+struct RowInfo { int j; double dt, be, sg; };
+
 __device__ int chuzr_decide(const Dev& D, Ctl* c, ArgMax v, ArgMax vL, int tot, int dtot, int top_ev, bool dual_chk,
-                            bool do_top, int it, bool learned, int phase) {
+                            bool do_top, int it, bool learned, int phase, const RowInfo* iw = nullptr,
+                            const RowInfo* il = nullptr) {
     int s_pidx = -1;
     if (do_top) c->iteration = it;
     c->top_done = 0;
@@ -368,7 +376,7 @@ __device__ int chuzr_decide(const Dev& D, Ctl* c, ArgMax v, ArgMax vL, int tot, 
     // margin; otherwise fall back to the DSE row.
     if (learned && top_ev == EV_NONE && !(dual_chk && dtot > 0) && pidx >= 0) {
         const int pl = (vL.i == INT_MAX || !(vL.w > 0.0)) ? -1 : vL.i;
-        const double sg = pl >= 0 ? 1.0 / (1.0 + exp(-(double)D.score[pl])) : 0.0;
+        const double sg = pl < 0 ? 0.0 : il ? il->sg : 1.0 / (1.0 + exp(-(double)D.score[pl]));
         if (pl >= 0 && sg >= D.learn_margin) { pidx = pl; c->learned_used += 1; }
         else c->learned_fallback += 1;
     }
@@ -383,11 +391,18 @@ __device__ int chuzr_decide(const Dev& D, Ctl* c, ArgMax v, ArgMax vL, int tot, 
         c->ninfeas = tot;
         c->p = -1; c->p_idx = -1;
         if (pidx >= 0) {
-            const int j = D.basis[pidx];
-            double dt;
-            var_infeas(D.type[j], D.x[j], D.lb[j], D.ub[j], &dt);
+            const RowInfo* ri = (iw && pidx == v.i) ? iw : (il && pidx == vL.i) ? il : nullptr;
+            int j;
+            double dt, be;
+            if (ri) {
+                j = ri->j; dt = ri->dt; be = ri->be;
+            } else {
+                j = D.basis[pidx];
+                var_infeas(D.type[j], D.x[j], D.lb[j], D.ub[j], &dt);
+                be = D.beta[pidx];
+            }
             c->p = j; c->p_idx = pidx; c->delta = dt; c->is_lower = dt < 0;
-            c->beta_p = D.beta[pidx];
+            c->beta_p = be;
         }
         if (tot == 0) raise_ev(c, EV_OPTIMAL, ST_PRICING);
         else if (pidx < 0) raise_ev(c, EV_NO_P, ST_PRICING);
@@ -480,11 +495,24 @@ __global__ void k_chuzr(Dev D) {
     }
 }
 
-// CHUZR in one CTA (dense mode): every thread scans m / BS positions, so no
-// partials, ticket or second pass; then the gather of rho = row p of B^-1.
+// CHUZR over one thread-block cluster of CZ_CL CTAs (dense mode).  Each CTA
+// scans its share of the positions (loads issued together) and the dual-check
+// slots, reduces them in one fused block reduction, and stores its winners,
+// counts and the scanning threads' data of the winning rows into rank 0's
+// shared memory; after a hardware cluster barrier rank 0 combines the CZ_CL
+// partials (selections and integer sums: order-independent), decides, and
+// stores the leaving position into every CTA's shared memory; after a second
+// barrier all CTAs gather their share of rho = row p of B^-1.  Spreading the
+// scattered loads of the scan and the gather over CZ_CL SMs is the point: one
+// SM's L2 bandwidth bounds the single-CTA form.  Ctl is written in this kernel
+// only by rank 0 after the first barrier, so the early exit below is taken by
+// every CTA alike and no CTA misses a barrier.
+constexpr int CZ_CL = 8, CZ_BS = 256;
 template <int BS>
-__global__ void __launch_bounds__(BS) k_chuzr_cta(Dev D) {
+__global__ void __launch_bounds__(BS) k_chuzr_cluster(Dev D) {
     pdl_enter();
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
     Ctl* c = D.ctl;
     if (halted(c)) return;
     const int phase = c->phase;
@@ -493,25 +521,127 @@ __global__ void __launch_bounds__(BS) k_chuzr_cta(Dev D) {
     bool dual_chk;
     chuzr_top(c, do_top, &it, &top_ev, &dual_chk);
     const bool learned = D.learned && phase == 2 && it >= D.learn_start;
+    constexpr int STRIDE = CZ_CL * BS;
+    const int t0 = rank * BS + (int)threadIdx.x;
     ArgMax best{-1.0, INT_MAX}, bestL{-1.0, INT_MAX};
+    RowInfo rw{-1, 0.0, 0.0, 0.0}, rl{-1, 0.0, 0.0, 0.0};
     int infeas = 0, dbad = 0;
     if (top_ev == EV_NONE) {
-        for (int i = threadIdx.x; i < D.m; i += BS) chuzr_row(D, i, phase, learned, best, bestL, infeas);
+        if (phase == 2) {
+            constexpr int RPT = 2;
+            const double mix = D.learn_mix;
+            for (int i0 = 0; i0 < D.m; i0 += STRIDE * RPT) {
+                int ii[RPT], jj[RPT];
+                double be[RPT];
+                float sc[RPT];
+#pragma unroll
+                for (int u = 0; u < RPT; ++u) {
+                    ii[u] = i0 + u * STRIDE + t0;
+                    const int ic = min(ii[u], D.m - 1);
+                    jj[u] = D.basis[ic];
+                    be[u] = D.beta[ic];
+                    sc[u] = learned ? D.score[ic] : 0.f;
+                }
+                unsigned char tt[RPT];
+                double xx[RPT], ll[RPT], uu[RPT];
+#pragma unroll
+                for (int u = 0; u < RPT; ++u) { tt[u] = D.type[jj[u]]; xx[u] = D.x[jj[u]]; ll[u] = D.lb[jj[u]]; uu[u] = D.ub[jj[u]]; }
+#pragma unroll
+                for (int u = 0; u < RPT; ++u) {
+                    if (ii[u] >= D.m) continue;
+                    // DSEPricing (tpp:470-501) + checkPrimalFeasible, as chuzr_row
+                    double dt;
+                    if (var_infeas(tt[u], xx[u], ll[u], uu[u], &dt) && fabs(dt) > 1e-8) {
+                        const double w = (dt * dt) / be[u];
+                        if (w > 0.0) {   // strict '>' against max_weight = 0
+                            if (better_max(best, ArgMax{w, ii[u]}).i == ii[u]) {
+                                best = ArgMax{w, ii[u]};
+                                rw = RowInfo{jj[u], dt, be[u], 0.0};
+                            }
+                            if (learned) {
+                                const double sg = 1.0 / (1.0 + exp(-(double)sc[u]));
+                                const double v = w * (mix + (1.0 - mix) * sg);
+                                if (v > 0.0 && better_max(bestL, ArgMax{v, ii[u]}).i == ii[u]) {
+                                    bestL = ArgMax{v, ii[u]};
+                                    rl = RowInfo{jj[u], dt, be[u], sg};
+                                }
+                            }
+                        }
+                    }
+                    infeas += var_primal_ok(tt[u], xx[u], ll[u], uu[u]) ? 0 : 1;
+                }
+            }
+        } else {
+            for (int i = t0; i < D.m; i += STRIDE) chuzr_row(D, i, phase, learned, best, bestL, infeas);
+        }
         if (dual_chk)
-            for (int i = threadIdx.x; i < D.n; i += BS) dbad += var_dual_bad(D.type[D.nonbasis[i]], D.d[D.nonbasis[i]]) ? 1 : 0;
+            for (int i = t0; i < D.n; i += STRIDE) dbad += var_dual_bad(D.type[D.nonbasis[i]], D.d[D.nonbasis[i]]) ? 1 : 0;
     }
-    best = block_argmax<BS>(best);
-    if (learned) bestL = block_argmax<BS>(bestL);
-    infeas = block_sum_int<BS>(infeas);
-    dbad = block_sum_int<BS>(dbad);
-    __shared__ int s_pidx;
-    if (threadIdx.x == 0) s_pidx = chuzr_decide(D, c, best, bestL, infeas, dbad, top_ev, dual_chk, do_top, it, learned, phase);
+    const int my_i = best.i, my_il = bestL.i;
+    // fused block reduction
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __shared__ double s_w[BS / 32], s_wl[BS / 32];
+    __shared__ int s_i[BS / 32], s_il[BS / 32], s_inf[BS / 32], s_db[BS / 32];
+    __shared__ int s_win, s_winl, s_pidx;
+    // rank 0's cluster partials
+    __shared__ ArgMax c_b[CZ_CL], c_bl[CZ_CL];
+    __shared__ int c_inf[CZ_CL], c_db[CZ_CL];
+    __shared__ RowInfo c_rw[CZ_CL], c_rl[CZ_CL];
+    for (int o = 16; o > 0; o >>= 1) {
+        best = better_max(best, ArgMax{__shfl_down_sync(FULL, best.w, o), __shfl_down_sync(FULL, best.i, o)});
+        bestL = better_max(bestL, ArgMax{__shfl_down_sync(FULL, bestL.w, o), __shfl_down_sync(FULL, bestL.i, o)});
+        infeas += __shfl_down_sync(FULL, infeas, o);
+        dbad += __shfl_down_sync(FULL, dbad, o);
+    }
+    if (lane == 0) { s_w[wid] = best.w; s_i[wid] = best.i; s_wl[wid] = bestL.w; s_il[wid] = bestL.i; s_inf[wid] = infeas; s_db[wid] = dbad; }
     __syncthreads();
-    if (s_pidx >= 0) {
-        const double* src = D.Binv + s_pidx;
+    if (wid == 0) {
+        const bool in = lane < BS / 32;
+        best = in ? ArgMax{s_w[lane], s_i[lane]} : ArgMax{-1.0, INT_MAX};
+        bestL = in ? ArgMax{s_wl[lane], s_il[lane]} : ArgMax{-1.0, INT_MAX};
+        infeas = in ? s_inf[lane] : 0;
+        dbad = in ? s_db[lane] : 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            best = better_max(best, ArgMax{__shfl_down_sync(FULL, best.w, o), __shfl_down_sync(FULL, best.i, o)});
+            bestL = better_max(bestL, ArgMax{__shfl_down_sync(FULL, bestL.w, o), __shfl_down_sync(FULL, bestL.i, o)});
+            infeas += __shfl_down_sync(FULL, infeas, o);
+            dbad += __shfl_down_sync(FULL, dbad, o);
+        }
+        if (lane == 0) {
+            s_win = best.i; s_winl = bestL.i;
+            *cl.map_shared_rank(&c_b[rank], 0) = best;
+            *cl.map_shared_rank(&c_bl[rank], 0) = bestL;
+            *cl.map_shared_rank(&c_inf[rank], 0) = infeas;
+            *cl.map_shared_rank(&c_db[rank], 0) = dbad;
+        }
+    }
+    __syncthreads();
+    // the threads that scanned this CTA's winning rows hand their data to rank 0
+    if (my_i != INT_MAX && my_i == s_win) *cl.map_shared_rank(&c_rw[rank], 0) = rw;
+    if (my_il != INT_MAX && my_il == s_winl) *cl.map_shared_rank(&c_rl[rank], 0) = rl;
+    cl.sync();
+    if (rank == 0 && threadIdx.x == 0) {
+        ArgMax v{-1.0, INT_MAX}, vL{-1.0, INT_MAX};
+        int tot = 0, dtot = 0, rv = -1, rvl = -1;
+        for (int r = 0; r < CZ_CL; ++r) {
+            if (better_max(v, c_b[r]).i != v.i) { v = c_b[r]; rv = r; }
+            if (better_max(vL, c_bl[r]).i != vL.i) { vL = c_bl[r]; rvl = r; }
+            tot += c_inf[r];
+            dtot += c_db[r];
+        }
+        const bool info = phase == 2 && top_ev == EV_NONE;
+        const int pidx = chuzr_decide(D, c, v, vL, tot, dtot, top_ev, dual_chk, do_top, it, learned, phase,
+                                      (info && v.i != INT_MAX && rv >= 0) ? &c_rw[rv] : nullptr,
+                                      (info && learned && vL.i != INT_MAX && rvl >= 0) ? &c_rl[rvl] : nullptr);
+        for (int r = 0; r < CZ_CL; ++r) *cl.map_shared_rank(&s_pidx, r) = pidx;
+    }
+    cl.sync();
+    const int p = s_pidx;
+    if (p >= 0) {
+        const double* src = D.Binv + p;
         const size_t M = D.m;
-#pragma unroll 4
-        for (int r = threadIdx.x; r < D.m; r += BS) D.rho[r] = src[(size_t)r * M];
+        for (int r = t0; r < D.m; r += STRIDE) D.rho[r] = src[(size_t)r * M];
     }
 }
 
@@ -667,6 +797,73 @@ __device__ int rt_select(const Dev& D, double sgn_a) {
     return result;
 }
 
+// Last block of the pivot-row kernels: combine the per-block candidate counts
+// and (t1, i1, t2) minima in block order, then CHUZC part 2 + the BFRT loop
+// (cudaDualSimplex.cpp:484-549), writing q, theta and delta_bfrt to Ctl.
+template <int BS>
+__device__ void pivot_row_finish(const Dev& D, Ctl* c, int phase, double sgn_a) {
+    __shared__ int s_tot, s_q, s_fast;
+    int tot = 0;
+    Min2 g{CUDART_INF, INT_MAX, CUDART_INF};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
+        tot += __ldcg(&D.redi[b]);
+        g = comb_min2(g, Min2{__ldcg(&D.red[2 * b]), __ldcg(&D.redi[gridDim.x + b]), __ldcg(&D.red[2 * b + 1])});
+    }
+    tot = block_sum_int<BS>(tot);
+    g = block_min2<BS>(g);
+    if (threadIdx.x == 0) {
+        s_tot = tot;
+        c->ncand = tot;
+        if (tot == 0) raise_ev(c, phase == 2 ? EV_UNBOUNDED : EV_P1_BLOCK, ST_RATIO);
+        else if (phase == 2) c->unbound_checked = 0;
+        // fast path: no second candidate within the tie window of the first
+        // minimiser, so the ordered scan (rt_select) would return it unchanged
+        s_fast = (g.i1 != INT_MAX && g.t2 > g.t1 + RT_WINDOW) ? g.i1 : -1;
+    }
+    __syncthreads();
+    if (s_tot == 0) return;
+    // CHUZC part 2 + BFRT
+    double delta = fabs(c->delta);
+    int remaining = s_tot;
+    int q_idx = -1;
+    bool first_pass = true;
+    while (true) {
+        const int qi = (first_pass && s_fast >= 0) ? s_fast : rt_select<BS>(D, sgn_a);
+        first_pass = false;
+        if (threadIdx.x == 0) s_q = qi;
+        __syncthreads();
+        if (s_q < 0) break;          // nothing takeable (reference: uninitialised q)
+        q_idx = s_q;
+        if (phase != 2) break;
+        const int qv = D.nonbasis[q_idx];
+        if (D.type[qv] != BOXED) break;
+        const double span = (D.ub[qv] - D.lb[qv]) * fabs(sgn_a * __ldcg(&D.alpha[q_idx]));
+        if (delta - span <= 0) break;
+        delta -= span;
+        __syncthreads();
+        if (threadIdx.x == 0) __stcg(&D.theta_arr[q_idx], CUDART_NAN);   // F.erase(q_idx)
+        --remaining;
+        __syncthreads();
+        if (remaining == 0) break;
+    }
+    if (threadIdx.x == 0) {
+        if (q_idx < 0) { c->err = 1; raise_ev(c, EV_ERROR, ST_RATIO); return; }
+        const int qv = D.nonbasis[q_idx];
+        c->q = qv; c->q_idx = q_idx;
+        c->theta = D.d[qv] / __ldcg(&D.alpha[q_idx]);
+        c->delta_bfrt = (c->is_lower ? -1.0 : 1.0) * delta;
+        if (phase == 1) {
+            // infisibilityCorr(q) (tpp:614-625) on d before the update
+            const unsigned char t = D.type[qv];
+            const double dq = D.d[qv];
+            double corr = 0;
+            if ((t == UPPER || t == FREE) && dq > EPS_D) corr = 1;
+            else if ((t == LOWER || t == FREE) && dq < -EPS_D) corr = -1;
+            c->dz = corr;   // phase 1 reuses dz for the correction term
+        }
+    }
+}
+
 // alpha_i = sum_e a_e rho[row_e] in CSC order (matrix.cpp:273-286), fused with the
 // candidate test; the last block selects q (CHUZC) and runs the BFRT loop
 // (cudaDualSimplex.cpp:484-549).  Phase 1 uses phase1SetRatioTestCandidates.
@@ -740,66 +937,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
         D.red[2 * blockIdx.x + 1] = mm.t2;
     }
     if (!last_block(&c->tickets[3])) return;
-    __shared__ int s_tot, s_q, s_fast;
-    int tot = 0;
-    Min2 g{CUDART_INF, INT_MAX, CUDART_INF};
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) {
-        tot += __ldcg(&D.redi[b]);
-        g = comb_min2(g, Min2{__ldcg(&D.red[2 * b]), __ldcg(&D.redi[gridDim.x + b]), __ldcg(&D.red[2 * b + 1])});
-    }
-    tot = block_sum_int<BS>(tot);
-    g = block_min2<BS>(g);
-    if (threadIdx.x == 0) {
-        s_tot = tot;
-        c->ncand = tot;
-        if (tot == 0) raise_ev(c, phase == 2 ? EV_UNBOUNDED : EV_P1_BLOCK, ST_RATIO);
-        else if (phase == 2) c->unbound_checked = 0;
-        // fast path: no second candidate within the tie window of the first
-        // minimiser, so the ordered scan (rt_select) would return it unchanged
-        s_fast = (g.i1 != INT_MAX && g.t2 > g.t1 + RT_WINDOW) ? g.i1 : -1;
-    }
-    __syncthreads();
-    if (s_tot == 0) return;
-    // CHUZC part 2 + BFRT
-    double delta = fabs(c->delta);
-    int remaining = s_tot;
-    int q_idx = -1;
-    bool first_pass = true;
-    while (true) {
-        const int qi = (first_pass && s_fast >= 0) ? s_fast : rt_select<BS>(D, sgn_a);
-        first_pass = false;
-        if (threadIdx.x == 0) s_q = qi;
-        __syncthreads();
-        if (s_q < 0) break;          // nothing takeable (reference: uninitialised q)
-        q_idx = s_q;
-        if (phase != 2) break;
-        const int qv = D.nonbasis[q_idx];
-        if (D.type[qv] != BOXED) break;
-        const double span = (D.ub[qv] - D.lb[qv]) * fabs(sgn_a * __ldcg(&D.alpha[q_idx]));
-        if (delta - span <= 0) break;
-        delta -= span;
-        __syncthreads();
-        if (threadIdx.x == 0) __stcg(&D.theta_arr[q_idx], CUDART_NAN);   // F.erase(q_idx)
-        --remaining;
-        __syncthreads();
-        if (remaining == 0) break;
-    }
-    if (threadIdx.x == 0) {
-        if (q_idx < 0) { c->err = 1; raise_ev(c, EV_ERROR, ST_RATIO); return; }
-        const int qv = D.nonbasis[q_idx];
-        c->q = qv; c->q_idx = q_idx;
-        c->theta = D.d[qv] / __ldcg(&D.alpha[q_idx]);
-        c->delta_bfrt = (c->is_lower ? -1.0 : 1.0) * delta;
-        if (phase == 1) {
-            // infisibilityCorr(q) (tpp:614-625) on d before the update
-            const unsigned char t = D.type[qv];
-            const double dq = D.d[qv];
-            double corr = 0;
-            if ((t == UPPER || t == FREE) && dq > EPS_D) corr = 1;
-            else if ((t == LOWER || t == FREE) && dq < -EPS_D) corr = -1;
-            c->dz = corr;   // phase 1 reuses dz for the correction term
-        }
-    }
+    pivot_row_finish<BS>(D, c, phase, sgn_a);
 }
 
 // ================================================================ dual update
@@ -1524,6 +1662,24 @@ static cudaError_t set_kernel_attributes(int cap) {
     return cudaSuccess;
 }
 
+// The dense CHUZR cluster, chained to the previous kernel like launch_pdl.
+static cudaError_t launch_chuzr_cluster(const Dev& D, cudaStream_t s) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(CZ_CL);
+    cfg.blockDim = dim3(CZ_BS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CZ_CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    return cudaLaunchKernelEx(&cfg, k_chuzr_cluster<CZ_BS>, D);
+}
+
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
     if (step != S_SCORE && !step_active(D, step)) return cudaSuccess;
     switch (step) {
@@ -1531,7 +1687,7 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
         case S_BINV: return launch_binv_update(D, 0, s);
         case S_SCORE: return launch_score(D, s);
         case S_CHUZR:
-            if (D.dense) { cudaError_t e = launch_pdl(k_chuzr_cta<1024>, dim3(1), dim3(1024), 0, s, D); if (e) return e; }
+            if (D.dense) { cudaError_t e = launch_chuzr_cluster(D, s); if (e) return e; }
             else { cudaError_t e = launch_pdl(k_chuzr<BS>, dim3(nblk(D.m > D.n ? D.m : D.n)), dim3(BS), g_smem_bytes(D.cap), s, D); if (e) return e; }
             break;
         case S_BTRAN_RHS: { cudaError_t e = launch_pdl(k_btran_rhs<BS>, dim3(nblk(D.k)), dim3(BS), 0, s, D, 0); if (e) return e; break; }
