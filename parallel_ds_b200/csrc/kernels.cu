@@ -940,6 +940,82 @@ __global__ void k_pivot_row(Dev D, int mode) {
     pivot_row_finish<BS>(D, c, phase, sgn_a);
 }
 
+// Serial part of the dual update, in one CTA once every slot is updated: the
+// dense-mode FTRAN/BTRAN pivot check, d_p = -theta, d_q = 0, the ordered flip
+// list, the column change and delta_z, and the eta-mode entering column.  tot:
+// flips found by the slot pass (valid in thread 0).
+template <int BS>
+__device__ void dual_update_finish(const Dev& D, Ctl* c, int phase, double theta, int tot) {
+    if (D.dense && threadIdx.x == 0) {
+        // the reference's FTRAN/BTRAN pivot check (cudaDualSimplex.cpp:555)
+        const double aqp = __ldcg(&D.alpha_q[c->p_idx]);
+        const double apq = D.alpha[c->q_idx];
+        if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
+        else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
+    }
+    __shared__ int s_nf;
+    if (threadIdx.x == 0) {
+        s_nf = tot;
+        c->nflips = tot;
+        D.d[c->p] = -theta;
+        D.d[c->q] = 0.0;
+        if (phase == 1) c->z_phase1 = c->z_phase1 - theta * c->f_p;
+    }
+    __syncthreads();
+    // entering column a_q as a dense row vector (clear the previous one first);
+    // the eta-file FTRAN reads it, dense mode does not
+    const int pq = D.dense ? -1 : c->prev_q;
+    if (pq >= 0) {
+        if (pq < D.n) { for (int e = D.cptr[pq] + threadIdx.x; e < D.cptr[pq + 1]; e += BS) D.aq_dense[D.crow[e]] = 0.0; }
+        else if (threadIdx.x == 0) D.aq_dense[pq - D.n] = 0.0;
+    }
+    __syncthreads();
+    const int q = c->q;
+    if (!D.dense) {
+        if (q < D.n) { for (int e = D.cptr[q] + threadIdx.x; e < D.cptr[q + 1]; e += BS) D.aq_dense[D.crow[e]] = D.cval[e]; }
+        else if (threadIdx.x == 0) D.aq_dense[q - D.n] = 1.0;
+    }
+    if (threadIdx.x == 0) { c->prev_q = q; c->nrhs = (s_nf > 0) ? 3 : 2; }
+    if (s_nf == 0) { if (threadIdx.x == 0) c->dz = (phase == 2) ? 0.0 : c->dz; return; }
+    // ---- flips (rare): ordered lists, column change and delta_z in slot order
+    for (int r = threadIdx.x; r < D.m; r += BS) D.cc[r] = 0.0;
+    __syncthreads();
+    __shared__ int nlist;
+    if (threadIdx.x == 0) {
+        double dz = 0.0;
+        int nl = 0;
+        for (int s = 0; s < D.n; ++s) {
+            const unsigned char fl = __ldcg(&D.flip[s]);
+            if (!fl) continue;
+            const int j = D.nonbasis[s];
+            const double span = D.ub[j] - D.lb[j];
+            if (fl == 1) dz += D.cost[j] * span; else dz -= D.cost[j] * span;
+            D.flip_list[nl++] = (fl == 1) ? j : -(j + 1);
+        }
+        c->dz = dz;
+        nlist = nl;
+    }
+    __syncthreads();
+    // addSparseCol(low, +1) then addSparseCol(up, -1) (matrix.cpp:606-616)
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int u = 0; u < nlist; ++u) {
+            const int code = D.flip_list[u];
+            const bool low = code >= 0;
+            if ((pass == 0) != low) continue;
+            const int j = low ? code : -code - 1;
+            const double span = D.ub[j] - D.lb[j];
+            const double mult = low ? 1.0 : -1.0;
+            if (j < D.n) {
+                for (int e = D.cptr[j] + threadIdx.x; e < D.cptr[j + 1]; e += BS)
+                    D.cc[D.crow[e]] += D.cval[e] * span * mult;
+            } else if (threadIdx.x == 0) {
+                D.cc[j - D.n] += 1.0 * span * mult;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // ================================================================ dual update
 // d_j -= theta alpha_j over the nonbasic slots and the BFRT flip test
 // (cudaDualSimplex.cpp:564-593).  Last block: d_p = -theta, d_q = 0, the ordered
@@ -1004,77 +1080,10 @@ __global__ void k_dual_update(Dev D) {
     nf = block_sum_int<BS>(nf);
     if (threadIdx.x == 0) D.redi[blockIdx.x] = nf;
     if (!last_block(&c->tickets[4])) return;
-    if (D.dense && threadIdx.x == 0) {
-        // the reference's FTRAN/BTRAN pivot check (cudaDualSimplex.cpp:555)
-        const double aqp = __ldcg(&D.alpha_q[c->p_idx]);
-        const double apq = D.alpha[c->q_idx];
-        if (!(fabs(aqp) > 0.0) || isnan(aqp)) raise_ev(c, EV_ERROR, ST_FTRAN);
-        else if (fabs(aqp - apq) > EPS_R * (1 + fabs(aqp))) raise_ev(c, EV_MISMATCH, ST_FTRAN);
-    }
-    __shared__ int s_nf;
     int tot = 0;
     for (int b = threadIdx.x; b < (int)gridDim.x; b += BS) tot += __ldcg(&D.redi[b]);
     tot = block_sum_int<BS>(tot);
-    if (threadIdx.x == 0) {
-        s_nf = tot;
-        c->nflips = tot;
-        D.d[c->p] = -theta;
-        D.d[c->q] = 0.0;
-        if (phase == 1) c->z_phase1 = c->z_phase1 - theta * c->f_p;
-    }
-    __syncthreads();
-    // entering column a_q as a dense row vector (clear the previous one first);
-    // the eta-file FTRAN reads it, dense mode does not
-    const int pq = D.dense ? -1 : c->prev_q;
-    if (pq >= 0) {
-        if (pq < D.n) { for (int e = D.cptr[pq] + threadIdx.x; e < D.cptr[pq + 1]; e += BS) D.aq_dense[D.crow[e]] = 0.0; }
-        else if (threadIdx.x == 0) D.aq_dense[pq - D.n] = 0.0;
-    }
-    __syncthreads();
-    const int q = c->q;
-    if (!D.dense) {
-        if (q < D.n) { for (int e = D.cptr[q] + threadIdx.x; e < D.cptr[q + 1]; e += BS) D.aq_dense[D.crow[e]] = D.cval[e]; }
-        else if (threadIdx.x == 0) D.aq_dense[q - D.n] = 1.0;
-    }
-    if (threadIdx.x == 0) { c->prev_q = q; c->nrhs = (s_nf > 0) ? 3 : 2; }
-    if (s_nf == 0) { if (threadIdx.x == 0) c->dz = (phase == 2) ? 0.0 : c->dz; return; }
-    // ---- flips (rare): ordered lists, column change and delta_z in slot order
-    for (int r = threadIdx.x; r < D.m; r += BS) D.cc[r] = 0.0;
-    __syncthreads();
-    __shared__ int nlist;
-    if (threadIdx.x == 0) {
-        double dz = 0.0;
-        int nl = 0;
-        for (int s = 0; s < D.n; ++s) {
-            const unsigned char fl = __ldcg(&D.flip[s]);
-            if (!fl) continue;
-            const int j = D.nonbasis[s];
-            const double span = D.ub[j] - D.lb[j];
-            if (fl == 1) dz += D.cost[j] * span; else dz -= D.cost[j] * span;
-            D.flip_list[nl++] = (fl == 1) ? j : -(j + 1);
-        }
-        c->dz = dz;
-        nlist = nl;
-    }
-    __syncthreads();
-    // addSparseCol(low, +1) then addSparseCol(up, -1) (matrix.cpp:606-616)
-    for (int pass = 0; pass < 2; ++pass) {
-        for (int u = 0; u < nlist; ++u) {
-            const int code = D.flip_list[u];
-            const bool low = code >= 0;
-            if ((pass == 0) != low) continue;
-            const int j = low ? code : -code - 1;
-            const double span = D.ub[j] - D.lb[j];
-            const double mult = low ? 1.0 : -1.0;
-            if (j < D.n) {
-                for (int e = D.cptr[j] + threadIdx.x; e < D.cptr[j + 1]; e += BS)
-                    D.cc[D.crow[e]] += D.cval[e] * span * mult;
-            } else if (threadIdx.x == 0) {
-                D.cc[j - D.n] += 1.0 * span * mult;
-            }
-            __syncthreads();
-        }
-    }
+    dual_update_finish<BS>(D, c, phase, theta, tot);
 }
 
 // ====================================================================== FTRAN
@@ -1376,6 +1385,101 @@ __global__ void k_update(Dev D, int force) {
     }
 }
 
+// Dense-mode dual update and primal update in one thread-block cluster of
+// DU_CL CTAs (replaces k_dual_update + k_update there).  Pass 1: d_j -= theta
+// alpha_j and the BFRT flip test over the nonbasic slots
+// (cudaDualSimplex.cpp:564-593), and alpha_q = B^-1 a_q over the positions (the
+// entering column staged in shared memory).  Cluster barrier; rank 0 runs the
+// serial part (pivot check, flips, column change).  Cluster barrier; unless
+// that part raised an event, pass 2 updates x_B (or f in phase 1) over the
+// positions (cudaDualSimplex.cpp:254-309, :595-617).  Cluster barrier; rank 0
+// runs the bookkeeping tail (basis swap, objective, flips, trace).  The
+// barriers replace the global-memory tickets of the two-kernel form.  Ctl is
+// written here only by rank 0 between barriers, and every CTA reads what
+// decides an early exit right after a barrier, so all CTAs exit alike.
+constexpr int DU_CL = 16, DU_BS = 256;
+template <int BS>
+__global__ void __launch_bounds__(BS) k_dual_update_cluster(Dev D) {
+    pdl_enter();
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    Ctl* c = D.ctl;
+    if (halted(c)) return;
+    const int phase = c->phase;
+    const double theta = c->theta;
+    constexpr int STRIDE = DU_CL * BS;
+    const int t0 = rank * BS + (int)threadIdx.x;
+    int nf = 0;
+    for (int i = t0; i < D.n; i += STRIDE) {
+        const int j = D.nonbasis[i];
+        const double dj = D.d[j] - theta * D.alpha[i];
+        D.d[j] = dj;
+        unsigned char fl = 0;
+        if (phase == 2 && D.type[j] == BOXED) {
+            const double x = D.x[j];
+            if (fabs(x - D.lb[j]) < EPS_Z && dj < -EPS_D) fl = 1;
+            else if (fabs(x - D.ub[j]) < EPS_Z && dj > EPS_D) fl = 2;
+        }
+        D.flip[i] = fl;
+        nf += fl ? 1 : 0;
+    }
+    {   // alpha_q = B^-1 a_q, sixteen B^-1 loads in flight per thread
+        __shared__ int s_r[BS + 16];   // rows past the column's end read row 0 (not summed)
+        __shared__ double s_v[BS];
+        const int q = c->q;
+        const size_t M = D.m;
+        if (threadIdx.x < 16) s_r[BS + threadIdx.x] = 0;
+        for (int ib = rank * BS; ib < D.m; ib += STRIDE) {   // block-uniform
+            const int i = ib + (int)threadIdx.x;
+            double sq = 0.0;
+            if (q < D.n) {
+                const int e0 = D.cptr[q], e1 = D.cptr[q + 1];
+                for (int eb = e0; eb < e1; eb += BS) {
+                    const int cnt = min(BS, e1 - eb);
+                    __syncthreads();
+                    const bool in = (int)threadIdx.x < cnt;
+                    s_r[threadIdx.x] = in ? D.crow[eb + threadIdx.x] : 0;
+                    if (in) s_v[threadIdx.x] = D.cval[eb + threadIdx.x];
+                    __syncthreads();
+                    if (i < D.m) {
+                        for (int u0 = 0; u0 < cnt; u0 += 16) {
+                            double bv[16];
+#pragma unroll
+                            for (int u = 0; u < 16; ++u) bv[u] = D.Binv[(size_t)s_r[u0 + u] * M + i];
+#pragma unroll
+                            for (int u = 0; u < 16; ++u)
+                                if (u0 + u < cnt) sq += bv[u] * s_v[u0 + u];
+                        }
+                    }
+                }
+            } else if (i < D.m) {
+                sq = D.Binv[(size_t)(q - D.n) * M + i];
+            }
+            if (i < D.m) D.alpha_q[i] = sq;
+        }
+    }
+    __shared__ int c_nf[DU_CL];
+    nf = block_sum_int<BS>(nf);
+    if (threadIdx.x == 0) *cl.map_shared_rank(&c_nf[rank], 0) = nf;
+    cl.sync();
+    if (rank == 0) {
+        int tot = 0;
+        if (threadIdx.x == 0) for (int r = 0; r < DU_CL; ++r) tot += c_nf[r];
+        dual_update_finish<BS>(D, c, phase, theta, tot);
+    }
+    cl.sync();
+    if (halted(c)) return;   // pivot check failed: the host redoes this iteration's update
+    const UpdArgs u = update_args(D, c);
+    double dzc = 0.0;
+    for (int i = t0; i < D.m; i += STRIDE) dzc += update_position(D, u, i);
+    if (u.phase == 2 && u.nflips > 0) {
+        dzc = block_sum<BS>(dzc);
+        if (threadIdx.x == 0) D.red[rank] = dzc;
+    }
+    cl.sync();
+    if (rank == 0 && threadIdx.x == 0) update_tail(D, c, u, DU_CL);
+}
+
 // ================================================================ init helpers
 // setPrimalVars (tpp:74-101)
 __global__ void k_set_primal_vars(Dev D) {
@@ -1632,7 +1736,8 @@ bool step_active(const Dev& D, int step) {
         case S_SCORE: return score_step_active(D);
         case S_BTRAN_RHS: case S_FTRAN_K: return !D.dense && D.k > 0;
         case S_BTRAN_GEMV: case S_FTRAN_ASM: case S_ETA_APPLY: return !D.dense;
-        case S_FTRAN_DENSE: return false;   // dense FTRAN runs inside k_dual_update (mismatch path: launch_ftran_dense)
+        case S_FTRAN_DENSE: return false;   // dense FTRAN runs inside the dual update (mismatch path: launch_ftran_dense)
+        case S_UPDATE: return !D.dense;     // dense mode: inside k_dual_update_cluster (mismatch path: launch_update_forced)
         case S_BINV: return D.dense != 0;
         default: return true;
     }
@@ -1659,6 +1764,9 @@ static cudaError_t set_kernel_attributes(int cap) {
     if ((e = cudaFuncSetAttribute(k_btran_unit<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ftran_assemble<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_btran_dense_fix<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    // a 16-CTA cluster is above the portable size of 8
+    if ((e = cudaFuncSetAttribute(k_dual_update_cluster<DU_BS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+        return e;
     return cudaSuccess;
 }
 
@@ -1680,6 +1788,24 @@ static cudaError_t launch_chuzr_cluster(const Dev& D, cudaStream_t s) {
     return cudaLaunchKernelEx(&cfg, k_chuzr_cluster<CZ_BS>, D);
 }
 
+// The dense dual/primal update cluster, chained to the previous kernel like launch_pdl.
+static cudaError_t launch_dual_update_cluster(const Dev& D, cudaStream_t s) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(DU_CL);
+    cfg.blockDim = dim3(DU_BS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = DU_CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    return cudaLaunchKernelEx(&cfg, k_dual_update_cluster<DU_BS>, D);
+}
+
 cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
     if (step != S_SCORE && !step_active(D, step)) return cudaSuccess;
     switch (step) {
@@ -1698,7 +1824,12 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
             break;
         }
         case S_PIVOT_ROW: { cudaError_t e = launch_pdl(k_pivot_row<BS>, dim3(nblk(D.n)), dim3(BS), 0, s, D, 3); if (e) return e; break; }
-        case S_DUAL_UPDATE: { cudaError_t e = launch_pdl(k_dual_update<BS>, dim3(nblk(D.dense && D.m > D.n ? D.m : D.n)), dim3(BS), 0, s, D); if (e) return e; break; }
+        case S_DUAL_UPDATE: {
+            cudaError_t e = D.dense ? launch_dual_update_cluster(D, s)
+                                    : launch_pdl(k_dual_update<BS>, dim3(nblk(D.n)), dim3(BS), 0, s, D);
+            if (e) return e;
+            break;
+        }
         case S_FTRAN_K:
             if (D.k > 0) {
                 dim3 g(D.ftr_ntile, D.ftr_nchunk);
