@@ -51,6 +51,9 @@ constexpr int BATCH_ITERS = 100;
 // kernels of consecutive iterations are chained by programmatic dependencies,
 // so the boundary between iterations costs no graph launch.
 constexpr int GRAPH_UNROLL = 8;
+// Dense mode: largest probe residual of B^-1 (relative to 1 + |B^-1 v|) at
+// which the periodic rebuild is skipped.
+constexpr double DENSE_PROBE_TOL = 1e-10;
 
 // Blocks freed to the device's default memory pool stay cached for reuse
 // (release threshold: unlimited) instead of going back to the driver at each
@@ -113,6 +116,7 @@ struct Engine {
     DBuf<int> d_cpl_ptr, d_cpl_col;
     DBuf<double> d_cpl_val, d_Kinv, d_S, d_Pan, d_Wk, d_Winv;
     DBuf<int> d_rowpiv, d_piv_rows, d_ferr;
+    DBuf<unsigned long long> d_probe;
     DBuf<double> d_eta, d_Mtri;
     DBuf<int> d_eta_pos, d_ybt_pos;
     DBuf<double> d_rho, d_alpha, d_theta, d_ybt, d_btr_rhs, d_aq, d_cc, d_alpha_q, d_tau, d_dxb;
@@ -190,7 +194,12 @@ struct Engine {
         keep_pool_memory(opt.device);
         CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
         CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
-        CK(cudaStreamCreateWithFlags(&pd_stream, cudaStreamNonBlocking));
+        // the PDHG cluster needs sixteen SMs of one GPC at once: its stream gets
+        // the highest priority so that the block scheduler places it ahead of
+        // the iteration kernels queued on the main stream meanwhile
+        int prio_lo = 0, prio_hi = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+        CK(cudaStreamCreateWithPriority(&pd_stream, cudaStreamNonBlocking, prio_hi));
         CK(cudaEventCreateWithFlags(&pd_done, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&pd_go, cudaEventDisableTiming));
         CK(cudaEventCreate(&evr0)); CK(cudaEventCreate(&evr1));
@@ -274,12 +283,13 @@ struct Engine {
         d_btr_rhs.ensure(stream, m); d_aq.ensure(stream, m); d_cc.ensure(stream, m); d_alpha_q.ensure(stream, m); d_tau.ensure(stream, m); d_dxb.ensure(stream, m);
         for (auto& b : d_y0) b.ensure(stream, m);
         d_seta.ensure(stream, (size_t)MAX_FTRAN_RHS * cap);
-        const int nb = std::max((m + 255) / 256, (n + 255) / 256) + 8;
+        // per-block partials: 256-wide grids over m or n, and the 16-CTA clusters
+        const int nb = std::max(std::max((m + 255) / 256, (n + 255) / 256), 16) + 8;
         d_red.ensure(stream, 2 * nb); d_redi.ensure(stream, 4 * nb);
         d_flip.ensure(stream, n); d_flip_list.ensure(stream, n);
         d_tmp_rows.ensure(stream, m); d_tmp_rows2.ensure(stream, m); d_tmp_pos.ensure(stream, m); d_tmp_pos2.ensure(stream, m); d_h.ensure(stream, cap);
         d_ctl.ensure(stream, 1);
-        d_Winv.ensure(stream, 16 * 16); d_ferr.ensure(stream, 1);
+        d_Winv.ensure(stream, 16 * 16); d_ferr.ensure(stream, 1); d_probe.ensure(stream, 2);
         d_trace.ensure(stream, 2); d_trace_d.ensure(stream, 2);
         d_score.ensure(stream, m); d_enter_cnt.ensure(stream, N); d_entered_at.ensure(stream, N);
         dense = opt.dense_max_m > 0 && m <= opt.dense_max_m;
@@ -928,6 +938,26 @@ struct Engine {
         }
     }
 
+    // Dense mode, at the periodic rebuild: is the maintained B^-1 still accurate?
+    // The rank-1 updates drift slowly, so the rebuild (a k x k inversion, some
+    // milliseconds) is skipped while the probe residual |B (B^-1 v) - v|_max stays
+    // below DENSE_PROBE_TOL (1 + |B^-1 v|_max).  The per-iteration pivot check
+    // still forces a rebuild on any visible drift.  The eta-file path and
+    // strict_reference rebuild on every period, as the reference does.
+    bool inverse_accurate() {
+        if (!dense || opt.strict_reference) return false;
+        unsigned long long bits[2] = {0, 0};
+        CK(launch_binv_probe(D, d_tmp_rows.p, d_tmp_pos.p, d_probe.p, stream));
+        CK(cudaMemcpyAsync(bits, d_probe.p, sizeof(bits), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        double res, ymax;
+        std::memcpy(&res, &bits[0], sizeof(double));
+        std::memcpy(&ymax, &bits[1], sizeof(double));
+        if (opt.verbose)
+            fprintf(stderr, "[ds] it %d inverse probe residual %.3e |B^-1 v| %.3e\n", hc->iteration, res, ymax);
+        return res <= DENSE_PROBE_TOL * (1.0 + ymax);
+    }
+
     // remaining top-of-loop steps after a refactor at iteration it (reference order)
     void top_after_refactor() {
         pull();
@@ -986,7 +1016,8 @@ struct Engine {
                 case EV_ITER_LIMIT: status = DS_STATUS_ITER_LIMIT; return false;
                 case EV_REFACTOR_DUE:
                     clear_event(); push();
-                    refactor(); top_after_refactor();
+                    if (!inverse_accurate()) refactor();
+                    top_after_refactor();
                     ev = run_body_once();
                     continue;
                 case EV_DUALINF:

@@ -645,6 +645,42 @@ __global__ void __launch_bounds__(BS) k_chuzr_cluster(Dev D) {
     }
 }
 
+// Accuracy probe of the explicit inverse (dense mode): v_r = 1 + (r mod 7) / 8,
+// y = B^-1 v (k_dense_colsum), then the max-norm residual max_r |(B y)_r - v_r|
+// with B's columns taken at the basic positions (var_pos), each row summed in
+// CSR order; out[0] gets the residual and out[1] max_i |y_i|, as the bit
+// patterns of non-negative doubles (which order as integers; NaN counts as inf).
+__global__ void k_probe_fill(double* v, int m) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < m) v[r] = 1.0 + (double)(r % 7) * 0.125;
+}
+template <int BS>
+__global__ void k_basis_residual(Dev D, const double* y, const double* v, unsigned long long* out) {
+    const int r = blockIdx.x * BS + threadIdx.x;
+    double e = 0.0, a = 0.0;
+    if (r < D.m) {
+        double s = 0.0;
+        for (int k = D.rptr[r]; k < D.rptr[r + 1]; ++k) {
+            const int p = D.var_pos[D.rcol[k]];
+            if (p >= 0) s += D.rval[k] * y[p];
+        }
+        const int ps = D.var_pos[D.n + r];
+        if (ps >= 0) s += y[ps];
+        e = fabs(s - v[r]);
+        a = fabs(y[r]);
+        if (!(e <= CUDART_INF)) e = CUDART_INF;
+        if (!(a <= CUDART_INF)) a = CUDART_INF;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        e = fmax(e, __shfl_down_sync(0xffffffffu, e, o));
+        a = fmax(a, __shfl_down_sync(0xffffffffu, a, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[0], (unsigned long long)__double_as_longlong(e));
+        atomicMax(&out[1], (unsigned long long)__double_as_longlong(a));
+    }
+}
+
 // Standalone eta part of BTRAN for e_{p_idx} (exact DSE weight recomputation).
 template <int BS>
 __global__ void k_btran_unit(Dev D, int p_idx) {
@@ -864,6 +900,61 @@ __device__ void pivot_row_finish(const Dev& D, Ctl* c, int phase, double sgn_a) 
     }
 }
 
+// One nonbasic slot i of the pivot row: alpha_i = sum_e a_e rho[row_e] in CSC
+// order (matrix.cpp:273-286, mode bit 1) and the ratio-test candidate test
+// (mode bit 2), accumulated into the thread's count and (t1, i1, t2) minimum.
+__device__ __forceinline__ void pivot_row_slot(const Dev& D, int i, int mode, int phase, double sgn_a, int& ncand,
+                                               Min2& mm) {
+    const int j = D.nonbasis[i];
+    // the candidate test's operands depend only on j: load them with the dot's
+    unsigned char tj = 0;
+    double dj = 0.0, xj = 0.0, lj = 0.0, uj = 0.0;
+    if (mode & 2) { dj = D.d[j]; tj = D.type[j]; xj = D.x[j]; lj = D.lb[j]; uj = D.ub[j]; }
+    double acc = 0.0;
+    if (mode & 1) {
+        if (j < D.n) {
+            // the CSC order of the reference's dot (matrix.cpp:273-286), with the
+            // loads of sixteen nonzeros (the last batch predicated) issued before
+            // their products are summed
+            const int e1 = D.cptr[j + 1];
+            for (int e = D.cptr[j]; e < e1; e += 16) {
+                int rr[16];
+                double vv[16], pp[16];
+#pragma unroll
+                for (int u = 0; u < 16; ++u) {
+                    const bool ok = e + u < e1;
+                    rr[u] = ok ? D.crow[e + u] : 0;
+                    vv[u] = ok ? D.cval[e + u] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 16; ++u) pp[u] = D.rho[rr[u]];
+#pragma unroll
+                for (int u = 0; u < 16; ++u)
+                    if (e + u < e1) acc += vv[u] * pp[u];
+            }
+        } else {
+            acc += 1.0 * D.rho[j - D.n];
+        }
+        D.alpha[i] = acc;
+    } else {
+        acc = D.alpha[i];
+    }
+    if (mode & 2) {
+        const double a = sgn_a * acc;
+        bool cand;
+        if (phase == 2) cand = rt_candidate(a, tj, xj, lj, uj);
+        else cand = (dj >= 0 && a > EPS_A) || (dj <= 0 && a < -EPS_A);
+        double th = CUDART_NAN;
+        if (cand) {
+            ncand += 1;
+            const double tt = dj / a;
+            if (tt < INF_THETA) { th = tt; mm = comb_min2(mm, Min2{tt, i, CUDART_INF}); }   // NaN / >= INF never taken
+        }
+        D.theta_arr[i] = th;
+        D.cand[i] = cand ? 1 : 0;
+    }
+}
+
 // alpha_i = sum_e a_e rho[row_e] in CSC order (matrix.cpp:273-286), fused with the
 // candidate test; the last block selects q (CHUZC) and runs the BFRT loop
 // (cudaDualSimplex.cpp:484-549).  Phase 1 uses phase1SetRatioTestCandidates.
@@ -877,56 +968,7 @@ __global__ void k_pivot_row(Dev D, int mode) {
     const int i = blockIdx.x * BS + threadIdx.x;
     int ncand = 0;
     Min2 mm{CUDART_INF, INT_MAX, CUDART_INF};
-    if (i < D.n) {
-        const int j = D.nonbasis[i];
-        // the candidate test's operands depend only on j: load them with the dot's
-        unsigned char tj = 0;
-        double dj = 0.0, xj = 0.0, lj = 0.0, uj = 0.0;
-        if (mode & 2) { dj = D.d[j]; tj = D.type[j]; xj = D.x[j]; lj = D.lb[j]; uj = D.ub[j]; }
-        double acc = 0.0;
-        if (mode & 1) {
-            if (j < D.n) {
-                // the CSC order of the reference's dot (matrix.cpp:273-286), with the
-                // loads of sixteen nonzeros (the last batch predicated) issued before
-                // their products are summed
-                const int e1 = D.cptr[j + 1];
-                for (int e = D.cptr[j]; e < e1; e += 16) {
-                    int rr[16];
-                    double vv[16], pp[16];
-#pragma unroll
-                    for (int u = 0; u < 16; ++u) {
-                        const bool ok = e + u < e1;
-                        rr[u] = ok ? D.crow[e + u] : 0;
-                        vv[u] = ok ? D.cval[e + u] : 0.0;
-                    }
-#pragma unroll
-                    for (int u = 0; u < 16; ++u) pp[u] = D.rho[rr[u]];
-#pragma unroll
-                    for (int u = 0; u < 16; ++u)
-                        if (e + u < e1) acc += vv[u] * pp[u];
-                }
-            } else {
-                acc += 1.0 * D.rho[j - D.n];
-            }
-            D.alpha[i] = acc;
-        } else {
-            acc = D.alpha[i];
-        }
-        if (mode & 2) {
-            const double a = sgn_a * acc;
-            bool cand;
-            if (phase == 2) cand = rt_candidate(a, tj, xj, lj, uj);
-            else cand = (dj >= 0 && a > EPS_A) || (dj <= 0 && a < -EPS_A);
-            double th = CUDART_NAN;
-            if (cand) {
-                ncand = 1;
-                const double tt = dj / a;
-                if (tt < INF_THETA) { th = tt; mm = Min2{tt, i, CUDART_INF}; }   // NaN / >= INF never taken
-            }
-            D.theta_arr[i] = th;
-            D.cand[i] = cand ? 1 : 0;
-        }
-    }
+    if (i < D.n) pivot_row_slot(D, i, mode, phase, sgn_a, ncand, mm);
     ncand = block_sum_int<BS>(ncand);
     if (!(mode & 2)) return;
     mm = block_min2<BS>(mm);
@@ -937,6 +979,37 @@ __global__ void k_pivot_row(Dev D, int mode) {
         D.red[2 * blockIdx.x + 1] = mm.t2;
     }
     if (!last_block(&c->tickets[3])) return;
+    pivot_row_finish<BS>(D, c, phase, sgn_a);
+}
+
+// The pivot row of the iteration step in one thread-block cluster of PR_CL
+// CTAs (n <= PR_CL_MAX_N): the same slot work as k_pivot_row over a strided
+// slot range, per-CTA partials in global memory, then a hardware cluster
+// barrier instead of the last-block ticket, and rank 0 runs CHUZC + BFRT.  Ctl
+// is not written before the barrier, so every CTA takes the early exit alike.
+constexpr int PR_CL = 16, PR_BS = 256, PR_CL_MAX_N = 2 * PR_CL * PR_BS;
+template <int BS>
+__global__ void __launch_bounds__(BS) k_pivot_row_cluster(Dev D) {
+    pdl_enter();
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    Ctl* c = D.ctl;
+    if (halted(c)) return;
+    const int phase = c->phase;
+    const double sgn_a = (phase == 2) ? (c->is_lower ? -1.0 : 1.0) : (c->f_p > 0 ? -1.0 : 1.0);
+    int ncand = 0;
+    Min2 mm{CUDART_INF, INT_MAX, CUDART_INF};
+    for (int i = rank * BS + (int)threadIdx.x; i < D.n; i += PR_CL * BS) pivot_row_slot(D, i, 3, phase, sgn_a, ncand, mm);
+    ncand = block_sum_int<BS>(ncand);
+    mm = block_min2<BS>(mm);
+    if (threadIdx.x == 0) {
+        D.redi[rank] = ncand;
+        D.redi[PR_CL + rank] = mm.i1;
+        D.red[2 * rank] = mm.t1;
+        D.red[2 * rank + 1] = mm.t2;
+    }
+    cl.sync();
+    if (rank != 0) return;
     pivot_row_finish<BS>(D, c, phase, sgn_a);
 }
 
@@ -1767,6 +1840,8 @@ static cudaError_t set_kernel_attributes(int cap) {
     // a 16-CTA cluster is above the portable size of 8
     if ((e = cudaFuncSetAttribute(k_dual_update_cluster<DU_BS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
         return e;
+    if ((e = cudaFuncSetAttribute(k_pivot_row_cluster<PR_BS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
+        return e;
     return cudaSuccess;
 }
 
@@ -1786,6 +1861,24 @@ static cudaError_t launch_chuzr_cluster(const Dev& D, cudaStream_t s) {
     cfg.attrs = at;
     cfg.numAttrs = 2;
     return cudaLaunchKernelEx(&cfg, k_chuzr_cluster<CZ_BS>, D);
+}
+
+// The pivot-row cluster, chained to the previous kernel like launch_pdl.
+static cudaError_t launch_pivot_row_cluster(const Dev& D, cudaStream_t s) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(PR_CL);
+    cfg.blockDim = dim3(PR_BS);
+    cfg.stream = s;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = PR_CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    return cudaLaunchKernelEx(&cfg, k_pivot_row_cluster<PR_BS>, D);
 }
 
 // The dense dual/primal update cluster, chained to the previous kernel like launch_pdl.
@@ -1823,7 +1916,12 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
             if (e) return e;
             break;
         }
-        case S_PIVOT_ROW: { cudaError_t e = launch_pdl(k_pivot_row<BS>, dim3(nblk(D.n)), dim3(BS), 0, s, D, 3); if (e) return e; break; }
+        case S_PIVOT_ROW: {
+            cudaError_t e = (D.n <= PR_CL_MAX_N) ? launch_pivot_row_cluster(D, s)
+                                                 : launch_pdl(k_pivot_row<BS>, dim3(nblk(D.n)), dim3(BS), 0, s, D, 3);
+            if (e) return e;
+            break;
+        }
         case S_DUAL_UPDATE: {
             cudaError_t e = D.dense ? launch_dual_update_cluster(D, s)
                                     : launch_pdl(k_dual_update<BS>, dim3(nblk(D.n)), dim3(BS), 0, s, D);
@@ -2194,6 +2292,17 @@ cudaError_t launch_binv_update(const Dev& D, int force, cudaStream_t s) {
 cudaError_t launch_dense_ftran_vec(const Dev& D, const double* v, double* y, cudaStream_t s) {
     k_dense_colsum<BS><<<dim3(nblk(D.m), D.binv_chunks), BS, 0, s>>>(D, v, y, 0);
     count_launch(1);
+    LAUNCH_OK();
+    return cudaSuccess;
+}
+
+cudaError_t launch_binv_probe(const Dev& D, double* v, double* y, unsigned long long* out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    k_probe_fill<<<nblk(D.m), BS, 0, s>>>(v, D.m);
+    k_dense_colsum<BS><<<dim3(nblk(D.m), D.binv_chunks), BS, 0, s>>>(D, v, y, 0);
+    k_basis_residual<BS><<<nblk(D.m), BS, 0, s>>>(D, y, v, out);
+    count_launch(3);
     LAUNCH_OK();
     return cudaSuccess;
 }

@@ -102,6 +102,8 @@ cudaError_t launch_dense_rho(const Dev& D, int p_idx, cudaStream_t s);   // rho 
 cudaError_t launch_ftran_dense(const Dev& D, int check, int force, cudaStream_t s);
 cudaError_t launch_binv_update(const Dev& D, int force, cudaStream_t s);
 cudaError_t launch_dense_ftran_vec(const Dev& D, const double* v, double* y, cudaStream_t s);  // y = B^-1 v
+// out[0] = max |B (B^-1 v) - v| for a fixed probe v, out[1] = max |B^-1 v| (bit patterns of doubles)
+cudaError_t launch_binv_probe(const Dev& D, double* v, double* y, unsigned long long* out, cudaStream_t s);
 cudaError_t launch_dense_btran_vec(const Dev& D, const double* c, double* y, cudaStream_t s);  // y = B^-T c
 cudaError_t launch_dense_beta(const Dev& D, cudaStream_t s);             // exact DSE weights
 

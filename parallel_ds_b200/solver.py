@@ -117,7 +117,7 @@ class CudaDualSimplex:
     def __init__(self, problem, refactor_interval=100, max_iterations=2000000, pricing="dse",
                  strict_reference=False, seed=12345, device=0, learned_margin=0.5, learned_mix=0.05,
                  learned_pdhg_iters=4000, dense_max_m=4096, dense_refactor_interval=400,
-                 learned_start_iteration=-1, pdhg_cluster=1, model=None):
+                 learned_start_iteration=-1, pdhg_cluster=1, model=None, verbose=0):
         self.problem = problem
         self.L = _lib.lib()
         o = DsOptions()
@@ -135,6 +135,7 @@ class CudaDualSimplex:
         o.dense_refactor_interval = dense_refactor_interval
         o.learned_start_iteration = learned_start_iteration
         o.pdhg_cluster = pdhg_cluster
+        o.verbose = verbose
         self.opts = o
         self.h = C.c_void_p()
         rc = self.L.ds_create(C.byref(o), C.byref(self.h))
