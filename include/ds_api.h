@@ -81,12 +81,14 @@ typedef struct ds_options {
                                   update it by a rank-1 step per iteration instead of
                                   the eta file; exact DSE weights (default 4096;
                                   0 = always the eta file)                        */
-    int    dense_refactor_interval; /* dense mode: iterations between rebuilds of
-                                  B^-1 from a fresh factorisation (default 400; a
-                                  pivot mismatch rebuilds it at once as well)      */
+    int    dense_refactor_interval; /* dense mode: iterations between accuracy checks
+                                  of B^-1 (default 400): a probe residual
+                                  |B (B^-1 v) - v| above 1e-10 (1 + |B^-1 v|)
+                                  rebuilds it from a fresh factorisation; a pivot
+                                  mismatch rebuilds it at once as well             */
     int    learned_start_iteration; /* learned pricing: iterations before this one use
                                   DSE while the PDHG warm start runs on a second
-                                  stream (default -1 = m/8; 0 = wait for it first) */
+                                  stream (default -1 = 7m/20; 0 = wait for it first) */
     int    pdhg_cluster;       /* 1: run the PDHG warm start inside one 16-CTA thread-
                                   block cluster when the LP fits its shared memory
                                   (default 1); 0: always the launch-per-step graph */

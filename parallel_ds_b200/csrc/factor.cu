@@ -137,19 +137,20 @@ __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double*
     }
 }
 
-// S[P, j] <- Winv S[P, j] for every column j outside the panel.
+// S[P, j] <- Winv S[P, j] for every column j outside the panel: a group of
+// GJ_NB threads per column, thread a loading pivot row a's entry and forming
+// row a of the product (the sum over b in order, as a single thread would).
 __global__ void k_gj_rows(double* S, int k, int c0, int w, const int* piv_rows, const double* Winv) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= k || (j >= c0 && j < c0 + w)) return;
-    double v[GJ_NB], o[GJ_NB];
+    const int j = (int)((blockIdx.x * blockDim.x + threadIdx.x) / GJ_NB);
+    const int a = (int)(threadIdx.x % GJ_NB);
+    const unsigned mask = 0xffffu << (threadIdx.x & 16);   // this column's half-warp
+    if (j >= k || (j >= c0 && j < c0 + w)) return;        // whole groups leave together
     double* col = S + (size_t)j * k;
-    for (int a = 0; a < w; ++a) v[a] = col[piv_rows[c0 + a]];
-    for (int a = 0; a < w; ++a) {
-        double s = 0.0;
-        for (int b = 0; b < w; ++b) s += Winv[a * GJ_NB + b] * v[b];
-        o[a] = s;
-    }
-    for (int a = 0; a < w; ++a) col[piv_rows[c0 + a]] = o[a];
+    const int pr = (a < w) ? piv_rows[c0 + a] : 0;
+    const double va = (a < w) ? col[pr] : 0.0;
+    double s = 0.0;
+    for (int b = 0; b < w; ++b) s += Winv[a * GJ_NB + b] * __shfl_sync(mask, va, b, GJ_NB);
+    if (a < w) col[pr] = s;
 }
 
 // 32 x 32 tiles: rows on threadIdx.x (coalesced in column-major S), columns on y.
@@ -222,7 +223,7 @@ cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s
         const int w = (k - c0 < GJ_NB) ? (k - c0) : GJ_NB;
         if (smem) k_gj_panel<512, true><<<1, 512, psh, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
         else k_gj_panel<512, false><<<1, 512, 0, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
-        k_gj_rows<<<(k + 127) / 128, 128, 0, s>>>(F.S, k, c0, w, F.piv_rows, F.Winv);
+        k_gj_rows<<<(k * GJ_NB + 255) / 256, 256, 0, s>>>(F.S, k, c0, w, F.piv_rows, F.Winv);
         dim3 g((k + 31) / 32, (k + 31) / 32), b(32, 32);
         k_gj_update<<<g, b, 0, s>>>(F.S, k, c0, w, F.Pan, F.rowpiv, F.piv_rows, F.Winv);
     }

@@ -1692,18 +1692,45 @@ __global__ void k_dot_cost_x(Dev D, double* out) {
 template <int BS>
 __global__ void k_phase1_init(Dev D, double* cc) {
     for (int r = threadIdx.x; r < D.m; r += BS) cc[r] = 0.0;
+    // 1) the dual infeasible slots in slot order, compacted by a block scan into
+    //    flip_list (scratch here): +(i+1) for inf_l, -(i+1) for inf_u
+    __shared__ int s_cnt, s_warp[BS / 32];
+    int* list = D.flip_list;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_cnt = 0;
     __syncthreads();
-    __shared__ double Zs;
-    if (threadIdx.x == 0) Zs = 0.0;
-    __syncthreads();
-    for (int pass = 0; pass < 2; ++pass) {   // inf_l (+1) first, then inf_u (-1)
-        for (int i = 0; i < D.n; ++i) {
+    for (int i0 = 0; i0 < D.n; i0 += BS) {
+        const int i = i0 + (int)threadIdx.x;
+        int code = 0;
+        if (i < D.n) {
             const int j = D.nonbasis[i];
             const unsigned char t = D.type[j];
             const double dj = D.d[j];
             const bool up = (t == UPPER || t == FREE) && dj > EPS_D;
             const bool lo = !up && (t == LOWER || t == FREE) && dj < -EPS_D;
-            if (!((pass == 0 && lo) || (pass == 1 && up))) continue;
+            code = lo ? i + 1 : up ? -(i + 1) : 0;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, code != 0);
+        if (lane == 0) s_warp[wid] = __popc(bal);
+        __syncthreads();
+        int before = s_cnt;
+        for (int w = 0; w < wid; ++w) before += s_warp[w];
+        if (code != 0) list[before + __popc(bal & ((1u << lane) - 1u))] = code;
+        __syncthreads();
+        if (threadIdx.x == 0) for (int w = 0; w < BS / 32; ++w) s_cnt += s_warp[w];
+        __syncthreads();
+    }
+    // 2) Z and the column sum in slot order, inf_l (+1) first, then inf_u (-1)
+    __shared__ double Zs;
+    if (threadIdx.x == 0) Zs = 0.0;
+    __syncthreads();
+    const int cnt = s_cnt;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int u = 0; u < cnt; ++u) {
+            const int code = list[u];
+            if ((pass == 0) != (code > 0)) continue;   // block-uniform
+            const int j = D.nonbasis[(code > 0 ? code : -code) - 1];
+            const double dj = D.d[j];
             const double mult = (pass == 0) ? 1.0 : -1.0;
             if (threadIdx.x == 0) Zs = (pass == 0) ? Zs + dj : Zs - dj;
             if (j < D.n) {
