@@ -409,7 +409,7 @@ def batch_arm(args, rank, world, local_rank):
         "e2e": {"value": e_solved / (e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e_ms / args.steps},
         "roofline": {"bound": "hbm", "kernel": "k_batch_solve", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": BATCH_TRAFFIC_PER_ALG_BYTE * alg_bytes,
                      "peak_source": "measured" if peaks else "fallback",
                      "algorithmic_bytes_per_launch": alg_bytes},
         "gpu_launches": int(launches),
@@ -445,6 +445,15 @@ def _status(code):
     return STATUS.get(code, str(code))
 
 
+# DRAM bytes (read + write) per launch from one ncu capture of the kernel:
+# profiles/dense_iteration_kernels_learned_m2000.md (k_binv_update, m=2000:
+# B^-1 read from DRAM cold under ncu, its writes still in L2 at kernel end) and
+# profiles/k_batch_solve_batched_256.md (151 GB DRAM for 211 GB algorithmic
+# bytes on 256 LPs; applied to a full batch in that proportion).
+NCU_TRAFFIC = {"k_binv_update": 32.062464e6}
+BATCH_TRAFFIC_PER_ALG_BYTE = 151.0 / 211.0
+
+
 def profile_roofline(lib, h):
     """Per-kernel device times measured by the engine's replay profiler."""
     import json as _j
@@ -458,7 +467,8 @@ def profile_roofline(lib, h):
     top = max(prof["kernels"], key=lambda k: k["share"])
     achieved = top["bytes"] / (top["avg_us"] * 1e-6) / 1e9
     return {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_source": "measured" if peaks else "fallback",
+            "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(top["name"]),
+            "peak_source": "measured" if peaks else "fallback",
             "kernels": prof["kernels"]}
 
 

@@ -194,12 +194,7 @@ struct Engine {
         keep_pool_memory(opt.device);
         CK(cudaEventCreate(&ev0)); CK(cudaEventCreate(&ev1));
         CK(cudaEventCreate(&evp0)); CK(cudaEventCreate(&evp1));
-        // the PDHG cluster needs sixteen SMs of one GPC at once: its stream gets
-        // the highest priority so that the block scheduler places it ahead of
-        // the iteration kernels queued on the main stream meanwhile
-        int prio_lo = 0, prio_hi = 0;
-        CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-        CK(cudaStreamCreateWithPriority(&pd_stream, cudaStreamNonBlocking, prio_hi));
+        CK(cudaStreamCreateWithFlags(&pd_stream, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&pd_done, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&pd_go, cudaEventDisableTiming));
         CK(cudaEventCreate(&evr0)); CK(cudaEventCreate(&evr1));
