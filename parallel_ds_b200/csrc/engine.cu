@@ -99,6 +99,7 @@ struct Engine {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     bool loaded = false;
+    bool binv_valid = false;   // dense mode: B^-1 was built for this LP at least once
 
     // host copy of the LP (computational form: N = n + m, slacks implicit in A)
     int m = 0, n = 0, N = 0;
@@ -305,6 +306,7 @@ struct Engine {
         CK(cudaMemsetAsync(d_Mtri.p, 0, sizeof(double) * cap * cap, stream));
         CK(cudaStreamSynchronize(stream));
         loaded = true;
+        binv_valid = false;
         status = DS_STATUS_UNSOLVED;
     }
 
@@ -532,7 +534,7 @@ struct Engine {
                 }
             fprintf(stderr, "[ds-check] refactor it %d k %d |Kinv K - I| %.3e (%.2f ms)\n", hc->iteration, k, worst, ms);
         }
-        if (dense) CK(launch_binv_build(D, stream));   // B^-1 of the new B0 (D.k set by sync_dev above)
+        if (dense) { CK(launch_binv_build(D, stream)); binv_valid = true; }   // B^-1 of the new B0 (D.k set by sync_dev above)
         hc->T = 0;
         hc->k = k;
         push();
@@ -711,7 +713,7 @@ struct Engine {
             if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); phase1_init(); }
             pull();
             if (hc->cycle > NEED_RESTART || hc->z_phase1 > INF_OBJ || std::isnan(hc->z_phase1)) phase1_init();
-            if (hc->iteration % hc->R == 0) refactor();
+            if (hc->iteration % hc->R == 0) refresh();
             pull(); clear_event(); push();
             CK(launch_count_dual_inf(D, stream));
             CK(launch_body(D, ST_PRICING, stream));
@@ -725,7 +727,7 @@ struct Engine {
                     pivots_at_nop == hc->pivots) { result = EV_P1_DUALINF; break; }
                 if (!hc->p1_found) pivots_at_nop = hc->pivots;
                 clear_event(); push();
-                refactor(); phase1_init(); init_beta(false);
+                refresh(); phase1_init(); init_beta(false);
                 if (blocked_any) { CK(cudaMemsetAsync(d_blocked.p, 0, N, stream)); blocked_any = false; }
                 st.restarts++;
                 continue;
@@ -735,7 +737,7 @@ struct Engine {
                 CK(cudaMemcpyAsync(d_blocked.p + hc->p, &one, 1, cudaMemcpyHostToDevice, stream));
                 blocked_any = true;
                 clear_event(); push();
-                refactor(); phase1_init();
+                refresh(); phase1_init();
                 st.restarts++;
                 continue;
             }
@@ -953,14 +955,23 @@ struct Engine {
         return res <= DENSE_PROBE_TOL * (1.0 + ymax);
     }
 
+    // A refactorisation wherever the solve only needs an accurate B^-1 for the
+    // current basis (periodic, restarts, phase changes): in dense mode it is
+    // skipped while the maintained inverse passes the probe.  A pivot mismatch
+    // and the explicit basis solves always refactorise.
+    void refresh() {
+        if (binv_valid && inverse_accurate()) return;
+        refactor();
+    }
+
     // remaining top-of-loop steps after a refactor at iteration it (reference order)
     void top_after_refactor() {
         pull();
         if (hc->iteration % NEED_RESTART == 0 && !dual_feasible()) {
-            refactor(); phase1(); dual_simplex_init(); st.restarts++;
+            refresh(); phase1(); dual_simplex_init(); st.restarts++;
         }
         pull();
-        if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); perturb_guard(); }
+        if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refresh(); dual_simplex_init(); perturb_guard(); }
     }
 
     // Perturbing the basic costs moves y = B^-T c_B and can leave nonbasic reduced
@@ -968,7 +979,7 @@ struct Engine {
     // until its next NEED_RESTART check.  Restore dual feasibility at once.
     void perturb_guard() {
         if (opt.strict_reference || dual_feasible()) return;
-        refactor(); phase1(); dual_simplex_init(); st.restarts++;
+        refresh(); phase1(); dual_simplex_init(); st.restarts++;
     }
 
     // Run the rest of the current iteration from pricing on (after a top event).
@@ -994,7 +1005,7 @@ struct Engine {
 
     // callDualSolver (cudaDualSimplex.cpp:396-655)
     bool phase2() {
-        refactor();
+        refresh();
         dual_simplex_init();
         pull();
         hc->cycle = 0; hc->unbound_checked = 0; clear_event();
@@ -1011,20 +1022,20 @@ struct Engine {
                 case EV_ITER_LIMIT: status = DS_STATUS_ITER_LIMIT; return false;
                 case EV_REFACTOR_DUE:
                     clear_event(); push();
-                    if (!inverse_accurate()) refactor();
+                    refresh();
                     top_after_refactor();
                     ev = run_body_once();
                     continue;
                 case EV_DUALINF:
                     clear_event(); push();
-                    refactor(); phase1(); dual_simplex_init(); st.restarts++;
+                    refresh(); phase1(); dual_simplex_init(); st.restarts++;
                     pull();
-                    if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refactor(); dual_simplex_init(); perturb_guard(); }
+                    if (!perturbed && hc->cycle > MAX_CYCLE) { perturb(); refresh(); dual_simplex_init(); perturb_guard(); }
                     ev = run_body_once();
                     continue;
                 case EV_PERTURB:
                     clear_event(); push();
-                    perturb(); refactor(); dual_simplex_init();
+                    perturb(); refresh(); dual_simplex_init();
                     perturb_guard();
                     ev = run_body_once();
                     continue;
@@ -1034,7 +1045,7 @@ struct Engine {
                     if (!opt.strict_reference && pivots_at_nop == hc->pivots) { status = DS_STATUS_OPTIMAL; return true; }
                     pivots_at_nop = hc->pivots;
                     clear_event(); push();
-                    refactor(); init_beta(false); phase1(); dual_simplex_init(); st.restarts++;
+                    refresh(); init_beta(false); phase1(); dual_simplex_init(); st.restarts++;
                     ev = run_until_event();
                     continue;
                 }
@@ -1042,7 +1053,7 @@ struct Engine {
                     pull();
                     if (hc->unbound_checked) { status = DS_STATUS_PRIMAL_INFEASIBLE; return false; }
                     hc->unbound_checked = 1; clear_event(); push();
-                    refactor(); init_beta(false); phase1(); dual_simplex_init(); st.restarts++;
+                    refresh(); init_beta(false); phase1(); dual_simplex_init(); st.restarts++;
                     pull(); hc->unbound_checked = 1; push();
                     ev = run_until_event();
                     continue;
@@ -1193,7 +1204,7 @@ struct Engine {
             CK(cudaEventRecord(evp1, stream));
         }
         try {
-            refactor();                      // initDualSimplex (cudaDualSimplex.cpp:20-81)
+            refresh();                       // initDualSimplex (cudaDualSimplex.cpp:20-81)
             if (perturb_needed()) perturb();  // presolve (tpp:5-30)
             init_beta(true);
             const int p1 = phase1();
@@ -1208,7 +1219,7 @@ struct Engine {
                     dual_simplex_init();
                     if (!ok || opt.strict_reference || dual_feasible()) break;
                     status = DS_STATUS_UNSOLVED;
-                    refactor();
+                    refresh();
                     if (phase1() == EV_P1_DUALINF) { status = DS_STATUS_DUAL_INFEASIBLE; break; }
                     CK(launch_set_primal_vars(D, stream));
                     ok = phase2();
