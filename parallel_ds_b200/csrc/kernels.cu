@@ -1090,9 +1090,10 @@ __device__ void dual_update_finish(const Dev& D, Ctl* c, int phase, double theta
 }
 
 // ================================================================ dual update
-// d_j -= theta alpha_j over the nonbasic slots and the BFRT flip test
-// (cudaDualSimplex.cpp:564-593).  Last block: d_p = -theta, d_q = 0, the ordered
-// flip list, the column change and delta_z, and the dense entering column.
+// Eta-file mode (dense mode runs k_dual_update_cluster): d_j -= theta alpha_j
+// over the nonbasic slots and the BFRT flip test (cudaDualSimplex.cpp:564-593).
+// Last block: d_p = -theta, d_q = 0, the ordered flip list, the column change
+// and delta_z, and the dense entering column.
 template <int BS>
 __global__ void k_dual_update(Dev D) {
     pdl_enter();
@@ -1114,41 +1115,6 @@ __global__ void k_dual_update(Dev D) {
         }
         D.flip[i] = fl;
         nf = fl ? 1 : 0;
-    }
-    if (D.dense && blockIdx.x * BS < D.m) {   // block-uniform
-        // dense mode: the iteration FTRAN alpha_q = B^-1 a_q rides on this grid.
-        // The entering column's nonzeros are staged in shared memory, so that
-        // every thread issues sixteen B^-1 loads before summing them in order.
-        __shared__ int s_r[BS + 16];   // rows past the column's end read row 0 (not summed)
-        __shared__ double s_v[BS];
-        const int q = c->q;
-        const size_t M = D.m;
-        double sq = 0.0;
-        if (threadIdx.x < 16) s_r[BS + threadIdx.x] = 0;
-        if (q < D.n) {
-            const int e0 = D.cptr[q], e1 = D.cptr[q + 1];
-            for (int eb = e0; eb < e1; eb += BS) {
-                const int cnt = min(BS, e1 - eb);
-                __syncthreads();
-                const bool in = (int)threadIdx.x < cnt;
-                s_r[threadIdx.x] = in ? D.crow[eb + threadIdx.x] : 0;
-                if (in) s_v[threadIdx.x] = D.cval[eb + threadIdx.x];
-                __syncthreads();
-                if (i < D.m) {
-                    for (int u0 = 0; u0 < cnt; u0 += 16) {
-                        double bv[16];
-#pragma unroll
-                        for (int u = 0; u < 16; ++u) bv[u] = D.Binv[(size_t)s_r[u0 + u] * M + i];
-#pragma unroll
-                        for (int u = 0; u < 16; ++u)
-                            if (u0 + u < cnt) sq += bv[u] * s_v[u0 + u];
-                    }
-                }
-            }
-        } else if (i < D.m) {
-            sq = D.Binv[(size_t)(q - D.n) * M + i];
-        }
-        if (i < D.m) D.alpha_q[i] = sq;
     }
     nf = block_sum_int<BS>(nf);
     if (threadIdx.x == 0) D.redi[blockIdx.x] = nf;
