@@ -6,7 +6,7 @@
 // operation order and built with -ffp-contract=off so that single operations
 // round exactly as the reference's unfused x86-64 code does.
 //
-// Departures, each guarded by or_options and documented in DESIGN.md:
+// Departures from the reference, each guarded by or_options:
 //   * PARDISO (src/cpu/matrix.cpp:530-583) is replaced by a dense LU with
 //     partial pivoting of the basis's structural block K = A[R', S]; slack
 //     columns of the basis are eliminated exactly (they are unit columns).
