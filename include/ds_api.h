@@ -130,6 +130,25 @@ int ds_load_csr(ds_solver* s, int m, int n,
                 const double* col_lb, const double* col_ub,
                 const double* row_lb, const double* row_ub);
 
+/* MPS input for callers without Clp: replaces Problem::readMps over
+ * ClpModel::readMps (problem.tpp:332-409).  Fixed or free format; the first N
+ * row is the objective (further N rows are dropped); RANGES, BOUNDS
+ * UP/LO/FX/FR/MI/PL/BV/LI/UI (integrality ignored), the first RHS/RANGES/BOUNDS
+ * set; |value| >= 1e30 is infinite (+-1e300 in the arrays); SC bounds and
+ * OBJSENSE MAX are rejected.  obj_offset receives the RHS of the objective
+ * row: reported objectives are c^T x - obj_offset, as problem.tpp:256 does with
+ * ClpModel::objectiveOffset.
+ * ds_mps_read: call once with the array pointers NULL for m, n and nnz, then
+ * with arrays of m+1, nnz, nnz, n, n, n, m, m entries.  Parse errors return
+ * DS_ERR_ARG with the message in ds_mps_last_error() (per host thread).
+ * ds_load_mps: parse and ds_load_csr in one call. */
+int ds_mps_read(const char* path, int* m, int* n, long long* nnz,
+                int* row_ptr, int* col_idx, double* val, double* c,
+                double* col_lb, double* col_ub, double* row_lb, double* row_ub,
+                double* obj_offset);
+int ds_load_mps(ds_solver* s, const char* path, double* obj_offset);
+const char* ds_mps_last_error(void);
+
 /* Load with explicit bound types: the reference's 8-argument Problem ctor
  * (problem.tpp:143-173) -- bound_type, range_type, costs, lower_range,
  * upper_range, lower_bound, upper_bound, A(CSR, matrix.cpp:21-36). */

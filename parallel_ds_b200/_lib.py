@@ -110,6 +110,10 @@ def lib():
         "ds_profile_solve": (C.c_int, [C.c_void_p, C.c_char_p, C.c_int]),
         "ds_gen_lp": (C.c_longlong, [C.POINTER(DsGenSpec), IP, IP, DP, DP, DP, C.c_longlong]),
         "ds_gen_batch_m": (C.c_int, [C.c_ulonglong, C.c_int, C.c_int, C.c_int]),
+        "ds_mps_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                  IP, IP, DP, DP, DP, DP, DP, DP, DP]),
+        "ds_load_mps": (C.c_int, [C.c_void_p, C.c_char_p, DP]),
+        "ds_mps_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         if hasattr(L, name):

@@ -102,6 +102,34 @@ class Problem:
         rt = [kind(a, b) for a, b in zip(row_lb, row_ub)]
         return cls(bt, rt, c, row_lb, row_ub, col_lb, col_ub, A)
 
+    @classmethod
+    def readMps(cls, filename):
+        """Problem::readMps (problem.tpp:332-409) without Clp: the library's MPS
+        reader (ds_mps_read) gives the CSR matrix, costs and bounds; bound types
+        are derived as readMps does, and the RHS of the objective row becomes the
+        offset that getSolution subtracts (problem.tpp:256, 408)."""
+        L = _lib.lib()
+        path = str(filename).encode()
+        m, n, nnz, off = C.c_int(), C.c_int(), C.c_longlong(), C.c_double()
+        rc = L.ds_mps_read(path, C.byref(m), C.byref(n), C.byref(nnz), None, None, None, None, None, None, None,
+                           None, C.byref(off))
+        if rc != 0:
+            raise DsError(rc, L.ds_mps_last_error().decode())
+        m, n, nnz = m.value, n.value, nnz.value
+        rp = np.zeros(m + 1, np.int32)
+        ci = np.zeros(max(nnz, 1), np.int32)
+        va = np.zeros(max(nnz, 1))
+        c, clb, cub, rlb, rub = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(m), np.zeros(m)
+        rc = L.ds_mps_read(path, C.byref(C.c_int()), C.byref(C.c_int()), C.byref(C.c_longlong()),
+                           ptr(rp, C.c_int), ptr(ci, C.c_int), ptr(va, C.c_double), ptr(c, C.c_double),
+                           ptr(clb, C.c_double), ptr(cub, C.c_double), ptr(rlb, C.c_double), ptr(rub, C.c_double),
+                           C.byref(off))
+        if rc != 0:
+            raise DsError(rc, L.ds_mps_last_error().decode())
+        p = cls.from_bounds(Matrix(va[:nnz], rp, ci[:nnz], m, n), c, clb, cub, rlb, rub)
+        p._offset = off.value
+        return p
+
     def transformToComputeForm(self):
         """Slack columns are appended inside the engine (problem.tpp:176-226)."""
         self.computational = True
