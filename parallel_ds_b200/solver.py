@@ -134,7 +134,58 @@ class Problem:
         """Slack columns are appended inside the engine (problem.tpp:176-226)."""
         self.computational = True
 
+    def checkWellScaled(self):
+        """Problem::checkWellScaled (problem.tpp:26-43): log10(max|a| / min|a|) < 2
+        over the stored nonzeros (False for an empty matrix, as there)."""
+        a = np.abs(self.A.val)
+        if a.size == 0:
+            return False
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return bool(np.log10(a.max() / a.min()) < 2)
+
+    def scale(self):
+        """Problem::scale (problem.tpp:46-103): each row divided by its largest
+        |a| (row bounds too), then each column by its largest |a| after that;
+        costs are divided and column bounds multiplied by the column factors, so
+        x_scaled = scale_cols * x.  getSolution maps x back and re-prices it with
+        the original costs.  The reference leaves scaling off (problem.tpp:396-400);
+        an empty row keeps factor 1 here (the reference would read past the row)."""
+        A = self.A
+        m, n = A.getSize()
+        val = A.val.copy()
+        rows = np.repeat(np.arange(m), np.diff(A.row_ptr))
+        self.scale_rows = np.ones(m)
+        amax = np.zeros(m)
+        np.maximum.at(amax, rows, np.abs(val))
+        nz = np.diff(A.row_ptr) > 0
+        self.scale_rows[nz] = amax[nz]
+        val = val / self.scale_rows[rows]
+        self.lower_range = self.lower_range / self.scale_rows
+        self.upper_range = self.upper_range / self.scale_rows
+        self.scale_cols = np.zeros(n)
+        np.maximum.at(self.scale_cols, A.col_id, np.abs(val))
+        sc = self.scale_cols[A.col_id]
+        val = np.where(sc != 0, val / np.where(sc != 0, sc, 1.0), val)
+        has = self.scale_cols != 0
+        safe = np.where(has, self.scale_cols, 1.0)
+        self.costs = np.where(has, self.costs / safe, self.costs)
+        self.upper_bound = np.where(has, self.upper_bound * safe, self.upper_bound)
+        self.lower_bound = np.where(has, self.lower_bound * safe, self.lower_bound)
+        self.A = Matrix(val, A.row_ptr, A.col_id, m, n)
+        self.scaled = True
+
     def getSolution(self):
+        """Problem::getSolution (problem.tpp:241-259): unscale the structurals and
+        re-price them with the original costs when scaled, then subtract the
+        objective offset."""
+        if getattr(self, "scaled", False):
+            n = self.A.n
+            has = self.scale_cols != 0
+            safe = np.where(has, self.scale_cols, 1.0)
+            x = np.asarray(self.solution.x, np.float64).copy()
+            x[:n] = np.where(has, x[:n] / safe, x[:n])
+            self.solution.x = x
+            self.solution.Z = float(np.where(has, self.costs * safe, self.costs) @ x[:n])
         self.solution.Z -= self._offset
         return self.solution
 
