@@ -15,7 +15,9 @@
 //   * strict_reference = 0 adds two guards: a restart-loop stop and a
 //     post-perturbation cleanup (phase 1 + phase 2 on the original costs when
 //     the perturbed optimum is dual infeasible; the reference's callPrimalSolver
-//     is an empty stub, baseDualSimplex.tpp:677-680).
+//     is an empty stub, baseDualSimplex.tpp:677-680);
+//   * strict_reference = 0 also crashes free structural columns into the start
+//     basis (crash_free_columns), as the engine does.
 #include "ds_oracle.h"
 
 #include <algorithm>
@@ -126,9 +128,53 @@ struct Oracle {
         basis.resize(m); nonbasis.resize(n); is_basic.assign(N, 0);
         for (int i = 0; i < n; ++i) nonbasis[i] = i;
         for (int i = 0; i < m; ++i) { basis[i] = i + n; is_basic[i + n] = 1; }
+        if (!opt.strict_reference) crash_free_columns();
         beta.assign(m, 0.0);
         x.assign(N, 0.0); d.assign(N, 0.0);
         gen.seed((unsigned)(opt.seed & 0xffffffffu) ^ (unsigned)(opt.seed >> 32));
+    }
+
+    // Departure (strict_reference = 0): a nonbasic free structural with a nonzero
+    // reduced cost is dual infeasible, and the reference's phase 1 can leave one
+    // behind (then "optimal" at a dual infeasible basis).  Before the solve each
+    // free structural column takes the place of a slack whose row has a finite
+    // bound, chosen by partial pivoting on the columns eliminated so far
+    // (largest |entry|, lowest row on ties, pivots below 1e-9 of the column's
+    // largest entry refused), which keeps the structural block nonsingular.  At
+    // most CRASH_MAX columns; a free basic variable never leaves the basis.
+    static constexpr int CRASH_MAX = 512;
+    void crash_free_columns() {
+        std::vector<int> cols;
+        for (int j = 0; j < n && (int)cols.size() < CRASH_MAX; ++j)
+            if (type[j] == FREE && cptr[j + 1] > cptr[j]) cols.push_back(j);
+        if (cols.empty()) return;
+        std::vector<char> used(m, 0);
+        std::vector<std::vector<double>> elim;   // eliminated columns (dense over rows)
+        std::vector<int> prow;                   // their pivot rows
+        for (int j : cols) {
+            std::vector<double> v(m, 0.0);
+            for (int e = cptr[j]; e < cptr[j + 1]; ++e) v[crow[e]] = cval[e];
+            double vmax = 0.0;
+            for (int i = 0; i < m; ++i) vmax = std::max(vmax, std::fabs(v[i]));
+            for (size_t t = 0; t < elim.size(); ++t) {
+                const double f = v[prow[t]] / elim[t][prow[t]];
+                if (f != 0.0)
+                    for (int i = 0; i < m; ++i) v[i] -= f * elim[t][i];
+            }
+            int r = -1;
+            double best = 0.0;
+            for (int i = 0; i < m; ++i) {
+                if (used[i] || type[n + i] == FREE) continue;
+                const double a = std::fabs(v[i]);
+                if (a > best) { best = a; r = i; }
+            }
+            if (r < 0 || !(best > 1e-9 * vmax)) continue;
+            used[r] = 1;
+            elim.push_back(v);
+            prow.push_back(r);
+            basis[r] = j; is_basic[j] = 1;
+            nonbasis[j] = n + r; is_basic[n + r] = 0;
+        }
     }
 
     void tick() {

@@ -1137,6 +1137,49 @@ struct Engine {
     }
 
     // presolve + solve + postProcess (tpp:5-30, 123-180) with the cleanup guard
+    // A nonbasic free structural with a nonzero reduced cost is dual infeasible,
+    // and the reference's phase 1 can leave one behind (the solve then ends
+    // "optimal" at a dual infeasible basis).  Unless strict_reference is set,
+    // each free structural column (at most CRASH_MAX) first takes the place of a
+    // slack whose row has a finite bound, chosen by partial pivoting on the
+    // columns eliminated so far: largest |entry|, lowest row on ties, pivots below
+    // 1e-9 of the column's largest entry refused, so the structural block stays
+    // nonsingular.  A free basic variable never leaves the basis.
+    static constexpr int CRASH_MAX = 512;
+    void crash_free_columns(std::vector<int>& basis, std::vector<int>& nonbasis, std::vector<int>& var_pos) {
+        std::vector<int> cols;
+        for (int j = 0; j < n && (int)cols.size() < CRASH_MAX; ++j)
+            if (h_type[j] == FREE && h_cptr[j + 1] > h_cptr[j]) cols.push_back(j);
+        if (cols.empty()) return;
+        std::vector<char> used(m, 0);
+        std::vector<std::vector<double>> elim;
+        std::vector<int> prow;
+        for (int j : cols) {
+            std::vector<double> v(m, 0.0);
+            for (int e = h_cptr[j]; e < h_cptr[j + 1]; ++e) v[h_crow[e]] = h_cval[e];
+            double vmax = 0.0;
+            for (int i = 0; i < m; ++i) vmax = std::max(vmax, std::fabs(v[i]));
+            for (size_t t = 0; t < elim.size(); ++t) {
+                const double f = v[prow[t]] / elim[t][prow[t]];
+                if (f != 0.0)
+                    for (int i = 0; i < m; ++i) v[i] -= f * elim[t][i];
+            }
+            int r = -1;
+            double best = 0.0;
+            for (int i = 0; i < m; ++i) {
+                if (used[i] || h_type[n + i] == FREE) continue;
+                const double a = std::fabs(v[i]);
+                if (a > best) { best = a; r = i; }
+            }
+            if (r < 0 || !(best > 1e-9 * vmax)) continue;
+            used[r] = 1;
+            elim.push_back(std::move(v));
+            prow.push_back(r);
+            basis[r] = j; var_pos[j] = r;
+            nonbasis[j] = n + r; var_pos[n + r] = -(j + 1);
+        }
+    }
+
     void solve() {
         if (!loaded) throw CudaError("solve before load", DS_ERR_STATE);
         st = ds_stats{};
@@ -1149,6 +1192,7 @@ struct Engine {
         std::vector<int> basis(m), nonbasis(n), var_pos(N);
         for (int i = 0; i < n; ++i) { nonbasis[i] = i; var_pos[i] = -(i + 1); }
         for (int i = 0; i < m; ++i) { basis[i] = n + i; var_pos[n + i] = i; }
+        if (!opt.strict_reference) crash_free_columns(basis, nonbasis, var_pos);
         CK(cudaMemcpyAsync(d_basis.p, basis.data(), sizeof(int) * m, cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_nonbasis.p, nonbasis.data(), sizeof(int) * n, cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_var_pos.p, var_pos.data(), sizeof(int) * N, cudaMemcpyHostToDevice, stream));

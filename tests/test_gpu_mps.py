@@ -6,7 +6,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from test_mps import SAMPLE_SOLVE, highs_general, to_mps, write
+from test_mps import FREE1, FREE2, FREE3, SAMPLE, SAMPLE_SOLVE, highs_general, to_mps, typed, write
+from oracle import pyoracle as po
 from parallel_ds_b200 import _lib
 from parallel_ds_b200 import lp as L
 from parallel_ds_b200 import solver as S
@@ -14,10 +15,12 @@ from parallel_ds_b200 import solver as S
 pytestmark = pytest.mark.gpu
 
 
-def test_readmps_mirror_path(tmp_path):
+@pytest.mark.parametrize("text", [SAMPLE_SOLVE, SAMPLE])
+def test_readmps_mirror_path(tmp_path, text):
     """problem.readMps -> transformToComputeForm -> CudaDualSimplex -> getSolution:
-    the reported objective is c^T x minus the file's objective offset."""
-    f = write(tmp_path, SAMPLE_SOLVE)
+    the reported objective is c^T x minus the file's objective offset (SAMPLE has
+    a free column, which the solver's crash makes basic)."""
+    f = write(tmp_path, text)
     problem = S.Problem.readMps(f)
     problem.transformToComputeForm()
     solver = S.CudaDualSimplex(problem)
@@ -62,3 +65,18 @@ def test_mps_round_trip_solves_identically(tmp_path):
     assert s.status() == a["status"] == "optimal"
     assert sol.Z == a["objective"] and sol.iterations == a["iterations"]
     np.testing.assert_array_equal(sol.x[:lp["n"]], a["x"][:lp["n"]])
+
+
+@pytest.mark.parametrize("text", [FREE1, FREE2, FREE3])
+@pytest.mark.parametrize("dense", [0, 4096])
+def test_free_columns_gpu_vs_oracle_and_highs(tmp_path, text, dense):
+    p = S.Problem.readMps(write(tmp_path, text))
+    h = highs_general(p)
+    r = po.solve_typed(typed(p))
+    s = S.CudaDualSimplex(S.Problem.readMps(write(tmp_path, text)), dense_max_m=dense)
+    s.initDualSimplex()
+    s.presolve("minInfeas")
+    sol = s.solve()
+    assert s.status() == "optimal"
+    assert abs(sol.Z - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
+    assert abs(sol.Z - r["objective"]) <= 1e-12 * max(1.0, abs(h.fun))

@@ -173,11 +173,30 @@ def highs_general(p):
     return linprog(p.costs, A_ub=A_ub, b_ub=b_ub, bounds=bnd, method="highs-ds")
 
 
-# The sample without its free column: with X3 free, the reference's algorithm
-# (the oracle, and the GPU engine with it) stops at "primal infeasible" on this
-# LP while HiGHS finds -5.5; that is the solver's handling of a free nonbasic
-# structural, not the reader's.
+# The sample without its free column, and three-line LPs with free columns.
+# Free structural columns go through the solver's crash (default mode): the
+# reference's phase 1 alone (strict_reference) stops with a dual infeasible
+# basis on them -- "primal infeasible" on the sample, 0 instead of -5 on FREE1.
 SAMPLE_SOLVE = SAMPLE.replace(" FR BND       X3\n", "")
+FREE1 = "NAME a\nROWS\n N obj\n L r1\nCOLUMNS\n    x obj -1 r1 1\nRHS\n    RHS r1 5\nBOUNDS\n FR B x\nENDATA\n"
+FREE2 = ("NAME a\nROWS\n N obj\n L r1\n G r2\nCOLUMNS\n    x obj -1 r1 1\n    y obj 1 r1 1\n    y r2 1\n"
+         "RHS\n    RHS r1 5 r2 1\nBOUNDS\n FR B x\nENDATA\n")
+FREE3 = ("NAME a\nROWS\n N obj\n E r1\nCOLUMNS\n    x obj -1 r1 -1\n    y obj 2 r1 1\nRHS\n    RHS r1 3\n"
+         "BOUNDS\n FR B x\n UP B y 10\nENDATA\n")
+
+
+@pytest.mark.parametrize("text", [SAMPLE, FREE1, FREE2, FREE3])
+def test_free_columns_oracle_vs_highs(tmp_path, text):
+    p = S.Problem.readMps(write(tmp_path, text))
+    h = highs_general(p)
+    r = po.solve_typed(typed(p))
+    assert h.status == 0 and r["status"] == "optimal"
+    assert abs(r["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
+
+
+def test_free_column_strict_reference_keeps_the_reference_phase1(tmp_path):
+    r = po.solve_typed(typed(S.Problem.readMps(write(tmp_path, FREE1))), strict_reference=1)
+    assert r["status"] == "optimal" and r["objective"] == 0.0   # HiGHS: -5
 
 
 def test_parsed_sample_solves_to_highs_optimum(tmp_path):
