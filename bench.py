@@ -185,7 +185,9 @@ def our_arm(args, rank, world, local_rank):
     # ---- time to optimal, one LP alone on the GPU: learned vs plain on the same seeds
     tto = []
     h1 = new_handle()
-    for t in [lp for row in lps for lp in row][:args.tto_lps]:
+    tto_seeds = [3000 + rank * args.tto_lps + i for i in range(args.tto_lps)]
+    for x in tto_seeds:
+        t = L.typed(gen(args.workload, x))
         load(h1, t); solve(h1)
         a = dict(ms=stats(h1).solve_ms, it=stats(h1).iterations, obj=lib.ds_get_objective(h1),
                  st=_status(lib.ds_get_status(h1)), pdhg_ms=stats(h1).pdhg_ms)
@@ -198,14 +200,20 @@ def our_arm(args, rank, world, local_rank):
     tto_block = None
     if tto:
         ta, tb = sum(a["ms"] for a, _ in tto), sum(b["ms"] for _, b in tto)
+        ia, ib = sum(a["it"] for a, _ in tto), sum(b["it"] for _, b in tto)
+        ratios = sorted(b["ms"] / a["ms"] for a, b in tto)
+        # short on purpose: the whole JSON line must stay readable in a log tail
         tto_block = {
-            "lps": len(tto), "pricing": args.pricing,
-            "ms": [a["ms"] for a, _ in tto], "plain_ms": [b["ms"] for _, b in tto],
-            "iterations": [a["it"] for a, _ in tto], "plain_iterations": [b["it"] for _, b in tto],
-            "mean_ms": ta / len(tto), "plain_mean_ms": tb / len(tto), "speedup_vs_plain": tb / ta,
-            "pdhg_ms": [a.get("pdhg_ms", 0.0) for a, _ in tto],
+            "speedup_vs_plain": round(tb / ta, 4), "mean_ms": round(ta / len(tto), 3),
+            "plain_mean_ms": round(tb / len(tto), 3), "lps": len(tto), "pricing": args.pricing,
+            "iters_per_s": round(ia / (ta / 1e3), 1), "plain_iters_per_s": round(ib / (tb / 1e3), 1),
+            "mean_iterations": round(ia / len(tto), 1), "plain_mean_iterations": round(ib / len(tto), 1),
+            "per_lp_speedup_min_median_max": [round(ratios[0], 3), round(ratios[len(ratios) // 2], 3),
+                                              round(ratios[-1], 3)],
+            "mean_pdhg_ms": round(sum(a.get("pdhg_ms", 0.0) for a, _ in tto) / len(tto), 3),
             "max_obj_rel_err_vs_plain": max(abs(a["obj"] - b["obj"]) / max(1.0, abs(b["obj"])) for a, b in tto),
             "statuses": sorted({a["st"] for a, _ in tto} | {b["st"] for _, b in tto}),
+            "seeds": f"{tto_seeds[0]}..{tto_seeds[-1]}",
         }
 
     # ---- value: LPs resident in HBM, K steps of Cc concurrent solves
@@ -290,7 +298,7 @@ def our_arm(args, rank, world, local_rank):
         "data": "synthetic: seeded generator, N(0,1) entries, x0~U[0,1], b=A x0+U[0.1,1], c~U[0,1]",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": args.pricing,
                    "scorer": os.path.relpath(args.weights, ROOT) if learned else None,
-                   "lps_per_step": Cc, "seeds_rank0": seeds, "refactor_interval": 100,
+                   "lps_per_step": Cc, "seeds_rank0": f"{seeds[0][0]}..{seeds[-1][-1]}", "refactor_interval": 100,
                    "parallelism": f"replicas x{world}, {Cc} concurrent solves per GPU",
                    "l2": "256 MB buffer written between steps (flush); each step solves its LPs to optimality",
                    "step": f"{Cc} complete solves to optimality (status optimal), one host thread and CUDA "
@@ -298,7 +306,7 @@ def our_arm(args, rank, world, local_rank):
         "iters_per_s": iters / (t_ms / 1e3),
         "iterations": iters,
         "time_to_optimal": tto_block,
-        "lp_time_to_optimal_ms": lp_ms,
+        "lp_time_to_optimal_ms": {"mean": round(statistics.mean(lp_ms), 3), "max": round(max(lp_ms), 3)},
         "statuses": sorted({_status(x) for x in statuses}),
         "e2e": {"value": e_solved / (e_ms / 1e3), "unit": "LPs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": e_ms / K},
@@ -469,7 +477,8 @@ def profile_roofline(lib, h):
     return {"bound": "hbm", "kernel": top["name"], "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": NCU_TRAFFIC.get(top["name"]),
             "peak_source": "measured" if peaks else "fallback",
-            "kernels": prof["kernels"]}
+            "kernels": {k["name"]: {"avg_us": round(k["avg_us"], 2), "gbs": round(k["gbs"], 1),
+                                    "share": round(k["share"], 3)} for k in prof["kernels"]}}
 
 
 def cpu_sample(workload):
@@ -559,7 +568,7 @@ def main():
     ap.add_argument("--pricing", default="learned", choices=["dse", "learned"])
     ap.add_argument("--weights", default=os.path.join(ROOT, "parallel_ds_b200", "weights",
                                                       "scorer_m2000_n4000_d1.npz"))
-    ap.add_argument("--tto-lps", type=int, default=4, help="LPs timed alone, learned and plain")
+    ap.add_argument("--tto-lps", type=int, default=32, help="held-out LPs timed alone, learned and plain")
     ap.add_argument("--concurrency", type=int, default=8, help="LPs solved at once per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--solve-one", type=int, default=None, metavar="SEED",
