@@ -282,17 +282,24 @@ int ds_kernel_ratio_test(int n, int N, const int* nonbasis, const double* alpha,
 
 /* Ratio test that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot call cudaMalloc: a host framework that
- * owns all device memory through its own pool, a latency-critical loop where
- * cudaMalloc/cudaFree would stall the device, or a host callback, where CUDA
- * allocation calls are not allowed.  Same kernel and results as
- * ds_kernel_ratio_test, but every array argument is a DEVICE pointer the caller
- * owns (type: one byte per variable, DS_* codes) and the outputs are host
- * scalars.  Scratch lives in a fixed array of about 0.6 MB that every GPU
- * loading this library holds until exit; n > DS_NOALLOC_MAX_SLOTS returns
- * DS_ERR_CAPACITY.  The first call on a device looks up that array's device
- * address, so make it before any stream capture.  All calls share the array:
+ * owns all device memory through its own pool (a stray cudaMalloc breaks its
+ * accounting and can fail under its memory cap), or a latency-critical loop
+ * where cudaMalloc/cudaFree would stall the device.  Same kernel and results
+ * as ds_kernel_ratio_test, but every array argument is a DEVICE pointer the
+ * caller owns and the outputs are host scalars.  Note the type array: ONE BYTE
+ * per variable (DS_* codes as unsigned char), where ds_kernel_ratio_test takes
+ * an int per variable; passing int32 codes here is read as garbage types.
+ * Scratch lives in a fixed array of about 0.6 MB that every GPU loading this
+ * library holds until exit; n > DS_NOALLOC_MAX_SLOTS returns DS_ERR_CAPACITY.
+ * The first call on a device looks up that array's device address and keeps
+ * it for the life of the process, so make the first call before any stream
+ * capture begins, and do not call it again after resetting the device
+ * (cudaDeviceReset invalidates the kept address).  All calls share the array:
  * calls that overlap on the GPU (other threads, other streams) race.  stream
- * may be NULL; the call returns after its stream has synchronised. */
+ * may be NULL.  The call copies its result back and synchronises its stream
+ * before it returns, so it makes CUDA calls of its own: it must not be made
+ * from inside a host function queued on a stream (cudaLaunchHostFunc), where
+ * CUDA calls are not allowed. */
 #define DS_NOALLOC_MAX_SLOTS 65536
 int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, const double* alpha,
                                  double delta, int is_lower, const double* x, const double* d,

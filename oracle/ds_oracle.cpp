@@ -148,32 +148,57 @@ struct Oracle {
         for (int j = 0; j < n && (int)cols.size() < CRASH_MAX; ++j)
             if (type[j] == FREE && cptr[j + 1] > cptr[j]) cols.push_back(j);
         if (cols.empty()) return;
-        std::vector<char> used(m, 0);
-        std::vector<std::vector<double>> elim;   // eliminated columns (dense over rows)
-        std::vector<int> prow;                   // their pivot rows
+        // Sparse elimination: the work column w is zero outside `touched`, and the
+        // eliminated columns keep only the rows they touched.  Every operation and
+        // its order equal the dense restatement (zeros subtract nothing), so the
+        // chosen rows do not change; the cost is the eliminated columns' nonzeros,
+        // not k*m.
+        std::vector<char> used(m, 0), mark(m, 0);
+        std::vector<double> w(m, 0.0);
+        std::vector<int> touched;
+        std::vector<std::vector<int>> eidx;      // eliminated columns: rows ...
+        std::vector<std::vector<double>> eval;   // ... and values
+        std::vector<int> prow;
+        std::vector<double> pval;
         for (int j : cols) {
-            std::vector<double> v(m, 0.0);
-            for (int e = cptr[j]; e < cptr[j + 1]; ++e) v[crow[e]] = cval[e];
+            touched.clear();
             double vmax = 0.0;
-            for (int i = 0; i < m; ++i) vmax = std::max(vmax, std::fabs(v[i]));
-            for (size_t t = 0; t < elim.size(); ++t) {
-                const double f = v[prow[t]] / elim[t][prow[t]];
+            for (int e = cptr[j]; e < cptr[j + 1]; ++e) {
+                const int i = crow[e];
+                w[i] = cval[e];
+                if (!mark[i]) { mark[i] = 1; touched.push_back(i); }
+                vmax = std::max(vmax, std::fabs(cval[e]));
+            }
+            for (size_t t = 0; t < eidx.size(); ++t) {
+                const double f = w[prow[t]] / pval[t];
                 if (f != 0.0)
-                    for (int i = 0; i < m; ++i) v[i] -= f * elim[t][i];
+                    for (size_t u = 0; u < eidx[t].size(); ++u) {
+                        const int i = eidx[t][u];
+                        w[i] -= f * eval[t][u];
+                        if (!mark[i]) { mark[i] = 1; touched.push_back(i); }
+                    }
             }
             int r = -1;
             double best = 0.0;
-            for (int i = 0; i < m; ++i) {
+            for (int i : touched) {
                 if (used[i] || type[n + i] == FREE) continue;
-                const double a = std::fabs(v[i]);
-                if (a > best) { best = a; r = i; }
+                const double a = std::fabs(w[i]);
+                if (a > best || (a == best && a > 0.0 && i < r)) { best = a; r = i; }
             }
-            if (r < 0 || !(best > 1e-9 * vmax)) continue;
-            used[r] = 1;
-            elim.push_back(v);
-            prow.push_back(r);
-            basis[r] = j; is_basic[j] = 1;
-            nonbasis[j] = n + r; is_basic[n + r] = 0;
+            const bool take = r >= 0 && best > 1e-9 * vmax;
+            if (take) {
+                std::vector<int> ix(touched);
+                std::vector<double> vx(touched.size());
+                for (size_t u = 0; u < touched.size(); ++u) vx[u] = w[touched[u]];
+                used[r] = 1;
+                eidx.push_back(std::move(ix));
+                eval.push_back(std::move(vx));
+                prow.push_back(r);
+                pval.push_back(w[r]);
+                basis[r] = j; is_basic[j] = 1;
+                nonbasis[j] = n + r; is_basic[n + r] = 0;
+            }
+            for (int i : touched) { w[i] = 0.0; mark[i] = 0; }
         }
     }
 

@@ -1151,32 +1151,57 @@ struct Engine {
         for (int j = 0; j < n && (int)cols.size() < CRASH_MAX; ++j)
             if (h_type[j] == FREE && h_cptr[j + 1] > h_cptr[j]) cols.push_back(j);
         if (cols.empty()) return;
-        std::vector<char> used(m, 0);
-        std::vector<std::vector<double>> elim;
+        // Sparse elimination: the work column w is zero outside `touched`, and the
+        // eliminated columns keep only the rows they touched.  Every operation and
+        // its order equal the dense restatement (zeros subtract nothing), so the
+        // chosen rows do not change; the cost is the eliminated columns' nonzeros,
+        // not k*m.
+        std::vector<char> used(m, 0), mark(m, 0);
+        std::vector<double> w(m, 0.0);
+        std::vector<int> touched;
+        std::vector<std::vector<int>> eidx;      // eliminated columns: rows ...
+        std::vector<std::vector<double>> eval;   // ... and values
         std::vector<int> prow;
+        std::vector<double> pval;
         for (int j : cols) {
-            std::vector<double> v(m, 0.0);
-            for (int e = h_cptr[j]; e < h_cptr[j + 1]; ++e) v[h_crow[e]] = h_cval[e];
+            touched.clear();
             double vmax = 0.0;
-            for (int i = 0; i < m; ++i) vmax = std::max(vmax, std::fabs(v[i]));
-            for (size_t t = 0; t < elim.size(); ++t) {
-                const double f = v[prow[t]] / elim[t][prow[t]];
+            for (int e = h_cptr[j]; e < h_cptr[j + 1]; ++e) {
+                const int i = h_crow[e];
+                w[i] = h_cval[e];
+                if (!mark[i]) { mark[i] = 1; touched.push_back(i); }
+                vmax = std::max(vmax, std::fabs(h_cval[e]));
+            }
+            for (size_t t = 0; t < eidx.size(); ++t) {
+                const double f = w[prow[t]] / pval[t];
                 if (f != 0.0)
-                    for (int i = 0; i < m; ++i) v[i] -= f * elim[t][i];
+                    for (size_t u = 0; u < eidx[t].size(); ++u) {
+                        const int i = eidx[t][u];
+                        w[i] -= f * eval[t][u];
+                        if (!mark[i]) { mark[i] = 1; touched.push_back(i); }
+                    }
             }
             int r = -1;
             double best = 0.0;
-            for (int i = 0; i < m; ++i) {
+            for (int i : touched) {
                 if (used[i] || h_type[n + i] == FREE) continue;
-                const double a = std::fabs(v[i]);
-                if (a > best) { best = a; r = i; }
+                const double a = std::fabs(w[i]);
+                if (a > best || (a == best && a > 0.0 && i < r)) { best = a; r = i; }
             }
-            if (r < 0 || !(best > 1e-9 * vmax)) continue;
-            used[r] = 1;
-            elim.push_back(std::move(v));
-            prow.push_back(r);
-            basis[r] = j; var_pos[j] = r;
-            nonbasis[j] = n + r; var_pos[n + r] = -(j + 1);
+            const bool take = r >= 0 && best > 1e-9 * vmax;
+            if (take) {
+                std::vector<int> ix(touched);
+                std::vector<double> vx(touched.size());
+                for (size_t u = 0; u < touched.size(); ++u) vx[u] = w[touched[u]];
+                used[r] = 1;
+                eidx.push_back(std::move(ix));
+                eval.push_back(std::move(vx));
+                prow.push_back(r);
+                pval.push_back(w[r]);
+                basis[r] = j; var_pos[j] = r;
+                nonbasis[j] = n + r; var_pos[n + r] = -(j + 1);
+            }
+            for (int i : touched) { w[i] = 0.0; mark[i] = 0; }
         }
     }
 

@@ -3,13 +3,16 @@
 // Some callers of this library cannot call cudaMalloc: code that runs while a
 // host framework owns every byte of device memory through its own pool (a
 // stray cudaMalloc breaks its accounting and can fail under its memory cap),
-// code on a latency-critical path where cudaMalloc / cudaFree would stall the
-// device, and code inside host callbacks where CUDA allocation calls are not
-// allowed.  ds_kernel_ratio_test_noalloc runs the same ratio-test kernel as
+// and code on a latency-critical path where cudaMalloc / cudaFree would stall
+// the device.  ds_kernel_ratio_test_noalloc runs the same ratio-test kernel as
 // ds_kernel_ratio_test on device arrays the caller already owns, and keeps its
 // own scratch (candidate thetas and flags, per-block counts, the control block)
 // in the file-scope array below, which every GPU that loads the library holds
-// until the process exits.
+// until the process exits.  The call copies its result to the host and
+// synchronises its stream, so it is not for host functions queued on a stream
+// (they may make no CUDA calls).  The device address of the array is looked up
+// once per device and kept; a device reset (cudaDeviceReset) makes it stale, so
+// the entry point is not for processes that reset the device.
 #include <cstring>
 #include <mutex>
 

@@ -5,7 +5,8 @@ Sources (read as text; the reference's gtest targets do not build):
     (EXPECT_NEAR tolerance 1e-8, 1e-4 for Test4).
   * tests/test_math.cpp:12-49 -- 3x3 LU solve known answers (plain and transposed).
 
-Run in the build container:  python tests/golden/extract_reference_kats.py [reference_root]
+Run where the reference sources are:
+    python tests/golden/extract_reference_kats.py REFERENCE_ROOT
 The JSON it writes is committed; nothing at test time reads the reference.
 """
 import json
@@ -13,7 +14,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: extract_reference_kats.py REFERENCE_ROOT (the checkout of veret-v/parallel_ds)")
+REF = sys.argv[1]
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_kats.json")
 
 TYPES = {"Fixed": 0, "Free": 1, "Boxed": 2, "Upper": 3, "Lower": 4}

@@ -1,11 +1,13 @@
 """The allocation-free ratio test (ds_kernel_ratio_test_noalloc).
 
 It serves callers that cannot call cudaMalloc (a framework that owns device
-memory through its own pool, latency-critical loops, host callbacks).  Its
-scratch is a fixed array inside the library, shared by every call, so this
-checks two calls in a row against the allocating entry point
-ds_kernel_ratio_test on the same vectors (bit-exact, the tolerance the other
-ratio-test parity tests use), and that an oversize input is rejected.
+memory through its own pool, latency-critical loops where an allocation would
+stall the device).  Its scratch is a fixed array inside the library, shared by
+every call, so this checks two calls in a row against the allocating entry
+point ds_kernel_ratio_test on the same vectors (bit-exact, the tolerance the
+other ratio-test parity tests use), a call at exactly the size limit on a
+caller's stream, that a call leaves the device's free memory unchanged, and
+that an oversize input is rejected.
 This file is collected last on purpose."""
 import ctypes as C
 
@@ -47,19 +49,29 @@ def with_alloc(nonbasis, alpha, delta, is_lower, x, d, lb, ub, typ):
     return (q.value, qi.value, th.value, do.value, nc.value)
 
 
-def without_alloc(nonbasis, alpha, delta, is_lower, x, d, lb, ub, typ):
+def on_device(nonbasis, alpha, delta, is_lower, x, d, lb, ub, typ):
     import torch
     dev = torch.device("cuda")
     t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in
          dict(nb=nonbasis, a=alpha, x=x, d=d, lb=lb, ub=ub, typ=typ.astype(np.uint8)).items()}
     torch.cuda.synchronize()
+    return t, delta, is_lower
+
+
+def call_noalloc(dev_args, stream=None):
+    t, delta, is_lower = dev_args
     q, qi, nc = C.c_int(), C.c_int(), C.c_int()
     th, do = C.c_double(), C.c_double()
-    rc = lib().ds_kernel_ratio_test_noalloc(len(nonbasis), len(x), t["nb"].data_ptr(), t["a"].data_ptr(), delta,
-                                            is_lower, t["x"].data_ptr(), t["d"].data_ptr(), t["lb"].data_ptr(),
-                                            t["ub"].data_ptr(), t["typ"].data_ptr(), C.byref(q), C.byref(qi),
-                                            C.byref(th), C.byref(do), C.byref(nc), None)
+    rc = lib().ds_kernel_ratio_test_noalloc(t["nb"].numel(), t["x"].numel(), t["nb"].data_ptr(), t["a"].data_ptr(),
+                                            delta, is_lower, t["x"].data_ptr(), t["d"].data_ptr(),
+                                            t["lb"].data_ptr(), t["ub"].data_ptr(), t["typ"].data_ptr(),
+                                            C.byref(q), C.byref(qi), C.byref(th), C.byref(do), C.byref(nc),
+                                            stream)
     return rc, (q.value, qi.value, th.value, do.value, nc.value)
+
+
+def without_alloc(*args):
+    return call_noalloc(on_device(*args))
 
 
 def test_noalloc_matches_allocating_entry_point_twice():
@@ -69,6 +81,23 @@ def test_noalloc_matches_allocating_entry_point_twice():
         rc, got = without_alloc(*args)
         assert rc == 0
         assert got == with_alloc(*args)
+
+
+def test_noalloc_at_the_limit_on_a_caller_stream_allocates_nothing():
+    import torch
+    args = case(4, 65536, 4000)          # exactly DS_NOALLOC_MAX_SLOTS nonbasic slots
+    dev_args = on_device(*args)
+    want = with_alloc(*args)
+    stream = torch.cuda.Stream()
+    rc, got = call_noalloc(dev_args, C.c_void_p(stream.cuda_stream))   # warm: kernels loaded, address set up
+    assert rc == 0 and got == want
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rc, got = call_noalloc(dev_args, C.c_void_p(stream.cuda_stream))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert rc == 0 and got == want
+    assert free1 == free0
 
 
 def test_noalloc_rejects_oversize():
