@@ -429,20 +429,23 @@ def batch_cpu_sample(workload, seconds=15.0, threads=1, max_lps=4096):
     """The oracle solving the batch's first instances (generated before the
     clock starts) on `threads` host threads until about `seconds` have passed."""
     from concurrent.futures import ThreadPoolExecutor
+    from oracle import lpgen as G
     from oracle import pyoracle as po
-    from parallel_ds_b200 import lp as L
     cfg = BATCH[workload]
-    lps = [L.typed(L.batched_instance(cfg["seed"], i, cfg["m_lo"], cfg["m_hi"], cfg["density"]))
-           for i in range(min(max_lps, cfg["count"]))]
-    t0 = time.perf_counter()
+    total = min(max_lps, cfg["count"])
+    # instances from the oracle's restatement of the generator (bit-identical
+    # to the library's), made in chunks outside the timed solves
+    dt = 0.0
     done, statuses = 0, set()
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        while time.perf_counter() - t0 < seconds and done < len(lps):
-            chunk = lps[done:done + 4 * threads]
+        while dt < seconds and done < total:
+            chunk = [G.typed(G.batched_instance(cfg["seed"], i, cfg["m_lo"], cfg["m_hi"], cfg["density"]))
+                     for i in range(done, min(total, done + 4 * threads))]
+            t0 = time.perf_counter()
             for r in ex.map(po.solve_typed, chunk):
                 statuses.add(r["status"])
+            dt += time.perf_counter() - t0
             done += len(chunk)
-    dt = time.perf_counter() - t0
     return {"value": done / dt, "unit": "LPs/s", "cores": threads, "kind": "port",
             "sample": f"oracle solves the batch's first {done} instances ({sorted(statuses)}) on {threads} "
                       f"thread(s), {dt:.1f} s"}
@@ -500,14 +503,18 @@ def reference_arm(args):
     with DSE pricing) solving the GPU arm's LPs to optimality, one LP per host
     thread on all host cores."""
     from concurrent.futures import ThreadPoolExecutor
+    from oracle import lpgen as G
     from oracle import pyoracle as po
-    from parallel_ds_b200 import lp as L
     cores = os.cpu_count() or 1
     K, W = args.steps, args.warmup
     per_step = max(1, min(args.concurrency, cores))
-    lps = [[L.typed(gen(args.workload, 2000 + s * args.concurrency + c)) for c in range(per_step)]
+    # inputs from the oracle's restatement of the generator (bit-identical to
+    # the GPU arm's), so this arm maps no product library
+    ref_gen = {"learned": G.learned, "plain_small": G.plain_small,
+               "plain_large": lambda sd: G.generate(1, 50000, 100000, per_col=8, seed=sd)}[args.workload]
+    lps = [[G.typed(ref_gen(2000 + s * args.concurrency + c)) for c in range(per_step)]
            for s in range(K)]
-    po.solve_typed(L.typed(gen("plain_small", 1000)))      # warm-up: load the library, fault in pages
+    po.solve_typed(G.typed(G.plain_small(1000)))      # warm-up: load the library, fault in pages
     rs = []
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=per_step) as ex:

@@ -92,7 +92,18 @@ typedef struct ds_options {
     int    pdhg_cluster;       /* 1: run the PDHG warm start inside one 16-CTA thread-
                                   block cluster when the LP fits its shared memory
                                   (default 1); 0: always the launch-per-step graph */
+    int    factor_mode;        /* eta-file mode's factorisation of B0 (the reference's
+                                  cuDSS LU, cudaSparseMatrix.cpp:502-567):
+                                  DS_FACTOR_SPARSE (default) a sparse LU of the
+                                  structural block (singleton triangularisation,
+                                  Markowitz kernel LU on the device, level-scheduled
+                                  solves); DS_FACTOR_DENSE an explicit dense inverse
+                                  of the structural block (Gauss-Jordan).  Dense
+                                  mode (dense_max_m) always builds the dense inverse */
 } ds_options;
+
+#define DS_FACTOR_SPARSE 0
+#define DS_FACTOR_DENSE  1
 
 typedef struct ds_stats {
     int    iterations;         /* reference `iteration` counter (phase 1 + 2)      */
@@ -108,6 +119,12 @@ typedef struct ds_stats {
     double solve_ms;           /* device time of ds_solve (CUDA events)            */
     double refactor_ms;        /* device time spent refactorising                  */
     double pdhg_ms;            /* device time of the PDHG warm-start estimate      */
+    int    lu_kernel;          /* sparse LU, last factorisation: order of the bump's
+                                  kernel left by the singleton triangularisation  */
+    int    lu_dense;           /* ... order of the dense block left by the kernel's
+                                  Markowitz rounds                                */
+    int    lu_levels;          /* ... levels of the FTRAN plus the BTRAN program   */
+    int    lu_rounds;          /* ... Markowitz rounds of the kernel LU            */
 } ds_stats;
 
 typedef struct ds_solver ds_solver;

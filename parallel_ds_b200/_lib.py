@@ -15,6 +15,7 @@ ERRORS = {-1: "DS_ERR_ARG", -2: "DS_ERR_CUDA", -3: "DS_ERR_STATE", -4: "DS_ERR_S
 STATUS = {0: "unsolved", 1: "optimal", 2: "primal_infeasible", 3: "dual_infeasible",
           4: "iter_limit", 5: "error"}
 PRICING_DSE, PRICING_LEARNED = 0, 1
+FACTOR_SPARSE, FACTOR_DENSE = 0, 1
 GEN_DENSITY, GEN_PER_COL, GEN_BLOCK = 0, 1, 2
 NUM_FEATURES = 12
 MLP_NPARAMS = 64 * NUM_FEATURES + 64 + 64 * 64 + 64 + 64 + 1
@@ -26,7 +27,7 @@ class DsOptions(C.Structure):
                 ("stream", C.c_void_p), ("learned_margin", C.c_double), ("verbose", C.c_int),
                 ("learned_mix", C.c_double), ("learned_pdhg_iters", C.c_int), ("dense_max_m", C.c_int),
                 ("dense_refactor_interval", C.c_int), ("learned_start_iteration", C.c_int),
-                ("pdhg_cluster", C.c_int)]
+                ("pdhg_cluster", C.c_int), ("factor_mode", C.c_int)]
 
 
 class DsStats(C.Structure):
@@ -34,7 +35,8 @@ class DsStats(C.Structure):
                 ("restarts", C.c_int), ("perturbed", C.c_int), ("bfrt_flips", C.c_int),
                 ("learned_used", C.c_int), ("learned_fallback", C.c_int), ("bump_size", C.c_int),
                 ("kernel_launches", C.c_int), ("solve_ms", C.c_double), ("refactor_ms", C.c_double),
-                ("pdhg_ms", C.c_double)]
+                ("pdhg_ms", C.c_double), ("lu_kernel", C.c_int), ("lu_dense", C.c_int),
+                ("lu_levels", C.c_int), ("lu_rounds", C.c_int)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

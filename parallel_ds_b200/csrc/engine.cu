@@ -20,23 +20,13 @@
 
 #include "../../include/ds_api.h"
 #include "engine.cuh"
+#include "host_util.cuh"
 #include "kernels.cuh"
 #include "mlp.cuh"
 #include "pdhg.cuh"
+#include "sparse_factor.cuh"
 
 namespace ds {
-
-struct CudaError : std::runtime_error {
-    int code;
-    CudaError(const std::string& s, int c) : std::runtime_error(s), code(c) {}
-};
-
-#define CK(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess)                                                                \
-            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_), DS_ERR_CUDA); \
-    } while (0)
 
 constexpr double PERTURB_RATIO = 0.25;
 constexpr double PSI = 1e-5;
@@ -70,28 +60,6 @@ static void keep_pool_memory(int dev) {
     }
     done.push_back(dev);
 }
-
-template <typename T>
-struct DBuf {
-    // Stream-ordered device buffer.  A reallocation frees the old block in the
-    // owning stream's order (work already queued there that reads it finishes
-    // first) without the device-wide synchronisation of cudaFree, so solver
-    // handles growing their buffers do not stall one another; growth is
-    // geometric, so a solve whose factor grows reallocates a few times only.
-    T* p = nullptr;
-    size_t n = 0;
-    cudaStream_t s = nullptr;
-    void alloc(cudaStream_t st, size_t count) {
-        release();
-        if (count == 0) count = 1;
-        CK(cudaMallocAsync(&p, count * sizeof(T), st));
-        n = count;
-        s = st;
-    }
-    void ensure(cudaStream_t st, size_t count) { if (count > n) alloc(st, std::max(count, n + n / 2)); }
-    void release() { if (p) cudaFreeAsync(p, s); p = nullptr; n = 0; }
-    ~DBuf() { if (p) cudaFree(p); }      // handle teardown: its stream may already be gone
-};
 
 struct Engine {
     ds_options opt;
@@ -128,6 +96,8 @@ struct Engine {
     DBuf<unsigned> d_tile_tickets;
     DBuf<double> d_tmp_rows, d_tmp_rows2, d_tmp_pos, d_tmp_pos2, d_h;
     DBuf<Ctl> d_ctl;
+    SparseLU sflu;                         // eta-file mode's sparse factor of B0
+    SfInfo sfi;                            // its last factorisation
     DBuf<float> d_score, d_ftr_feat;
     // first-order warm-start evidence (pdhg.cu)
     DBuf<double> d_pd_c, d_pd_lo, d_pd_hi, d_pd_L, d_pd_U, d_pd_tau, d_pd_sigma;
@@ -229,6 +199,17 @@ struct Engine {
               const double* row_lb, const double* row_ub) {
         m = m_; n = n_; N = n + m;
         const int nnz = row_ptr[m];
+        // non-finite input would poison every later step (the reference has no
+        // check and iterates on NaN): matrix entries and costs must be finite,
+        // bounds may be infinite but not NaN
+        for (int e = 0; e < nnz; ++e)
+            if (!std::isfinite(val[e])) throw CudaError("matrix entry is not finite", DS_ERR_ARG);
+        for (int j = 0; j < n; ++j) {
+            if (!std::isfinite(c[j])) throw CudaError("cost is not finite", DS_ERR_ARG);
+            if (std::isnan(col_lb[j]) || std::isnan(col_ub[j])) throw CudaError("column bound is NaN", DS_ERR_ARG);
+        }
+        for (int i = 0; i < m; ++i)
+            if (std::isnan(row_lb[i]) || std::isnan(row_ub[i])) throw CudaError("row bound is NaN", DS_ERR_ARG);
         h_rptr.assign(row_ptr, row_ptr + m + 1);
         h_rcol.assign(col_idx, col_idx + nnz);
         h_rval.assign(val, val + nnz);
@@ -477,10 +458,13 @@ struct Engine {
         nnz_cpl = (long long)ccol.size();
         put(d_cpl_ptr, cptr); put(d_cpl_col, ccol);
         if (!cval.empty()) CK(cudaMemcpyAsync(d_cpl_val.p, cval.data(), cval.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-        const size_t kk = (size_t)std::max(k, 1) * std::max(k, 1);
-        d_Kinv.ensure(stream, kk); d_S.ensure(stream, kk);
-        d_Pan.ensure(stream, (size_t)std::max(k, 1) * 16); d_Wk.ensure(stream, (size_t)std::max(k, 1) * 16);
-        d_rowpiv.ensure(stream, std::max(k, 1)); d_piv_rows.ensure(stream, std::max(k, 1));
+        const bool sparse = !dense && opt.factor_mode == DS_FACTOR_SPARSE && k > 0;
+        if (!sparse) {
+            const size_t kk = (size_t)std::max(k, 1) * std::max(k, 1);
+            d_Kinv.ensure(stream, kk); d_S.ensure(stream, kk);
+            d_Pan.ensure(stream, (size_t)std::max(k, 1) * 16); d_Wk.ensure(stream, (size_t)std::max(k, 1) * 16);
+            d_rowpiv.ensure(stream, std::max(k, 1)); d_piv_rows.ensure(stream, std::max(k, 1));
+        }
         // FTRAN launch geometry for this k
         const int tile = 256;
         const int ntile = std::max(1, (k + tile - 1) / tile);
@@ -492,16 +476,42 @@ struct Engine {
         d_part.ensure(stream, (size_t)nchunk * MAX_FTRAN_RHS * std::max(k, 1));
         d_tile_tickets.ensure(stream, ntile);
         CK(cudaMemsetAsync(d_tile_tickets.p, 0, sizeof(unsigned) * ntile, stream));
+        D.sf.on = 0;
         sync_dev();
-        FactorBufs F{d_S.p, d_Pan.p, d_Wk.p, d_rowpiv.p, d_piv_rows.p, d_Winv.p, d_ferr.p, d_s_var.p, d_row_kidx.p};
-        CK(cudaEventRecord(evr0, stream));
-        CK(factor_bump(F, D, k, stream));
-        CK(cudaEventRecord(evr1, stream));
         int ferr = 0;
-        CK(cudaMemcpyAsync(&ferr, d_ferr.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CK(cudaStreamSynchronize(stream));
-        float ms = 0; cudaEventElapsedTime(&ms, evr0, evr1);
-        st.refactor_ms += ms;
+        float ms = 0;
+        if (sparse) {
+            // sparse LU: host triangularisation, device kernel LU, solve programs
+            SfInput in{m, n, k, h_cptr.data(), h_crow.data(), h_cval.data(), (long long)h_cptr[n],
+                       s_var.data(), s_pos.data(), rp_row.data(), row_kidx.data()};
+            const auto h0 = std::chrono::steady_clock::now();
+            SfInfo fi = sflu.factor(in, d_cval.p, stream, &D.sf);
+            sfi = fi;
+            const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count();
+            st.refactor_ms += host_ms;   // the whole factorisation, host stages included
+            st.lu_kernel = fi.km; st.lu_dense = fi.kd; st.lu_rounds = fi.rounds;
+            st.lu_levels = fi.lev_ft + fi.lev_bt;
+            if (opt.verbose >= 1)
+                fprintf(stderr, "[ds] sparse LU it %d: k %d kernel %d (sparse pivots %d in %d rounds, dense %d%s), "
+                        "L %d U %d, levels %d/%d, entries %lld/%lld, %.2f ms (device %.2f)\n", hc->iteration, k, fi.km,
+                        fi.ks, fi.rounds, fi.kd, fi.dense_fallback ? ", dense fallback" : "", fi.lnnz, fi.unnz,
+                        fi.lev_ft, fi.lev_bt, fi.ent_ft, fi.ent_bt, host_ms, fi.kernel_ms);
+            if (fi.singular) {
+                char msg[320];
+                snprintf(msg, sizeof(msg), "singular basis in refactorisation (iteration %d, k %d): %s", hc->iteration, k, fi.msg);
+                throw CudaError(msg, DS_ERR_NUMERIC);
+            }
+            sync_dev();
+        } else {
+            FactorBufs F{d_S.p, d_Pan.p, d_Wk.p, d_rowpiv.p, d_piv_rows.p, d_Winv.p, d_ferr.p, d_s_var.p, d_row_kidx.p};
+            CK(cudaEventRecord(evr0, stream));
+            CK(factor_bump(F, D, k, stream));
+            CK(cudaEventRecord(evr1, stream));
+            CK(cudaMemcpyAsync(&ferr, d_ferr.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            cudaEventElapsedTime(&ms, evr0, evr1);
+            st.refactor_ms += ms;
+        }
         if (k > 0 && ferr) {
             // diagnostics: duplicate basic variables, K columns without an R' entry
             std::vector<int> seen(N, 0);
@@ -517,7 +527,7 @@ struct Engine {
                      "duplicate basics %d, empty K columns %d)", hc->iteration, k, ferr - 1, dups, empty_cols);
             throw CudaError(msg, DS_ERR_NUMERIC);
         }
-        if (opt.verbose >= 3 && k > 0) {
+        if (opt.verbose >= 3 && k > 0 && !sparse) {
             // debug: || Kinv K - I ||_max on the host
             std::vector<double> Ki((size_t)k * k), Kd((size_t)k * k, 0.0);
             CK(cudaMemcpyAsync(Ki.data(), d_Kinv.p, sizeof(double) * k * k, cudaMemcpyDeviceToHost, stream));
@@ -627,7 +637,7 @@ struct Engine {
             return;
         }
         pull();
-        if (hc->T == 0) {            // every caller refactors first: B = B0
+        if (hc->T == 0 && !D.sf.on) {   // every caller refactors first: B = B0 (explicit Kinv)
             CK(launch_beta_exact(D, stream));
             CK(cudaStreamSynchronize(stream));
             return;
@@ -786,10 +796,15 @@ struct Engine {
             case S_SCORE: return 69 * M + 10248.0 * ((m + 127) / 128);
             case S_CHUZR: return 37 * M + 8 * Tt + 4 * Tt * Tt + (dual_check ? 13 * Nn : 0);
             case S_BTRAN_RHS: return 24.0 * nnz_S + 20 * K;
-            case S_BTRAN_GEMV: return 8 * K * K + 8 * K + 12 * M;
+            case S_BTRAN_GEMV:
+                if (D.sf.on)   // program entries (coefficient + slot), ops (slot, range, divisor), dense block, gather/scatter
+                    return 12.0 * sfi.ent_bt + 16.0 * sfi.op_bt + 8.0 * sfi.kd * sfi.kd + 24 * K + 12 * (M - K);
+                return 8 * K * K + 8 * K + 12 * M;
             case S_PIVOT_ROW: return 12.0 * ((double)h_rptr[m] - nnz_S) + 8 * K + 4 * Nn + 8 * (Nn - K) + 8 * M + 50 * Nn;
             case S_DUAL_UPDATE: return 30 * Nn + (dense ? (12.0 + 8 * M) * ((double)h_rptr[m] / n) + 8 * M : 0.0);
-            case S_FTRAN_K: return 8 * K * K + 16 * R * K + 8 * R * K * D.ftr_nchunk;
+            case S_FTRAN_K:
+                if (D.sf.on) return R * (12.0 * sfi.ent_ft + 16.0 * sfi.op_ft + 8.0 * sfi.kd * sfi.kd + 24 * K);
+                return 8 * K * K + 16 * R * K + 8 * R * K * D.ftr_nchunk;
             case S_FTRAN_ASM: return 20.0 * nnz_cpl + (M - K) * (4 + 16 * R) + 8 * R * Tt;
             case S_ETA_APPLY: return 8 * Tt * M + 16 * R * M;
             case S_UPDATE: return dense ? 44 * M : 60 * M + 8 * Tt + 4 * Tt * Tt;
@@ -1380,6 +1395,7 @@ void ds_default_options(ds_options* o) {
     o->dense_refactor_interval = 400;
     o->learned_start_iteration = -1;
     o->pdhg_cluster = 1;
+    o->factor_mode = DS_FACTOR_SPARSE;
 }
 
 const char* ds_version(void) { return "ds_b200 1.0 (sm_100a)"; }

@@ -85,6 +85,38 @@ struct Ctl {
     unsigned tickets[TICKETS];
 };
 
+// Sparse LU of the structural bump K (eta-file mode, sparse_factor.cu).  The
+// factor is a sequence of k pivots ("slots"): K's column singletons, the
+// Markowitz pivots of its kernel, a small dense block, then K's row singletons,
+// which puts K in block upper triangular form.  A B0 solve runs a program of
+// levels over one vector of k slots: the ops of a level are independent, and
+// each sets v[slot] = (v[slot] - sum_e coef_e * v[src_e]) / diag.
+struct SfProg {
+    int nlev;
+    const int* lvl_ptr;        // nlev + 1: op ranges
+    const int* lvl_kind;       // nlev: 0 sparse ops, 1 dense block (Sinv), 2 dense block (SinvT)
+    const int* op_slot;        // per op: the slot it sets
+    const int* op_ptr;         // nop + 1: entry ranges
+    const double* op_diag;     // per op: divisor (1.0 for ops that only subtract)
+    const int* ent_slot;       // per entry: source slot
+    const double* ent_coef;    // per entry: coefficient
+};
+struct SfDev {
+    int on;                    // 1: B0 solves use this factor instead of Kinv
+    int k;                     // slots (bump size)
+    int d0, kd;                // dense block: first slot, order
+    int smem;                  // 1: the slot vector fits in shared memory
+    const double* Sinv;        // kd x kd inverse of the dense block (column major)
+    const double* SinvT;       // its transpose
+    const int* slot_row;       // constraint row of the slot's pivot row
+    const int* slot_kcol;      // K column of the slot's pivot column
+    const int* slot_pos;       // basis position of the slot's pivot column
+    SfProg ft, bt;             // FTRAN and BTRAN programs
+    double* gvec;              // MAX_FTRAN_RHS * k slot vectors (when smem == 0)
+    double* gtmp;              // MAX_FTRAN_RHS * kd dense-block scratch
+};
+constexpr int SF_SMEM_SLOTS = 26624;   // 208 KB of doubles: slot vectors up to this size live in shared memory
+
 struct Dev {
     int m, n, N, cap;            // cap = eta file capacity
     int k;                       // bump size of the current factor
@@ -102,7 +134,8 @@ struct Dev {
     int* pos_kidx;                                              // m: position -> K column, -1 for slack
     int* row_slackpos;                                          // m: row -> slack position, -1 if in R'
     int* cpl_ptr; int* cpl_col; double* cpl_val;                // coupling A[R, S] by rows
-    double* Kinv;                                               // k*k column major
+    double* Kinv;                                               // k*k column major (dense factor)
+    SfDev sf;                                                   // sparse factor (eta-file mode)
     // eta file
     double* eta; int* eta_pos; double* Mtri;                    // Mtri holds G (row t: G[t][0..t-1])
     // work vectors

@@ -48,6 +48,7 @@ constexpr int GJ_SMEM_ROWS = 1600;
 template <int BS, bool SMEM>
 __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double* Wk_g, int* rowpiv,
                            int* piv_rows, double* Winv, int* err) {
+    if (*(volatile int*)err) return;   // an earlier panel found the matrix singular
     extern __shared__ double sh[];
     __shared__ double red_v[BS / 32];
     __shared__ int red_i[BS / 32];
@@ -140,7 +141,8 @@ __global__ void k_gj_panel(double* S, int k, int c0, int w, double* Pan, double*
 // S[P, j] <- Winv S[P, j] for every column j outside the panel: a group of
 // GJ_NB threads per column, thread a loading pivot row a's entry and forming
 // row a of the product (the sum over b in order, as a single thread would).
-__global__ void k_gj_rows(double* S, int k, int c0, int w, const int* piv_rows, const double* Winv) {
+__global__ void k_gj_rows(double* S, int k, int c0, int w, const int* piv_rows, const double* Winv, const int* err) {
+    if (*err) return;   // singular: the pivot rows of this panel were not all chosen
     const int j = (int)((blockIdx.x * blockDim.x + threadIdx.x) / GJ_NB);
     const int a = (int)(threadIdx.x % GJ_NB);
     const unsigned mask = 0xffffu << (threadIdx.x & 16);   // this column's half-warp
@@ -155,7 +157,8 @@ __global__ void k_gj_rows(double* S, int k, int c0, int w, const int* piv_rows, 
 
 // 32 x 32 tiles: rows on threadIdx.x (coalesced in column-major S), columns on y.
 __global__ void k_gj_update(double* S, int k, int c0, int w, const double* Pan, const int* rowpiv,
-                            const int* piv_rows, const double* Winv) {
+                            const int* piv_rows, const double* Winv, const int* err) {
+    if (*err) return;
     __shared__ double sp[32][GJ_NB + 1];   // Pan rows of the tile
     __shared__ double sq[GJ_NB][33];       // S[P, tile columns] or Winv
     const int i = blockIdx.x * 32 + threadIdx.x;
@@ -193,19 +196,19 @@ __global__ void k_gj_update(double* S, int k, int c0, int w, const double* Pan, 
 }
 
 // Kinv(c, piv_rows[c2]) = S(piv_rows[c], c2)
-__global__ void k_gj_permute(const double* S, int k, const int* piv_rows, double* Kinv) {
+__global__ void k_gj_permute(const double* S, int k, const int* piv_rows, double* Kinv, const int* err) {
+    if (*err) return;
     const int c = blockIdx.x * 32 + threadIdx.x;
     const int c2 = blockIdx.y * 32 + threadIdx.y;
     if (c >= k || c2 >= k) return;
     Kinv[(size_t)c + (size_t)piv_rows[c2] * k] = S[(size_t)piv_rows[c] + (size_t)c2 * k];
 }
 
-cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s) {
+// Gauss-Jordan inverse of the k x k matrix in F.S (column major), written to out.
+cudaError_t gj_inverse(const FactorBufs& F, int k, double* out, cudaStream_t s) {
     if (k == 0) return cudaSuccess;
-    const size_t kk = (size_t)k * k;
-    k_fill_zero<<<1184, 256, 0, s>>>(F.S, kk);
-    k_build_K<<<(k + 255) / 256, 256, 0, s>>>(D.cptr, D.crow, D.cval, F.s_var, F.row_kidx, k, F.S);
     cudaMemsetAsync(F.rowpiv, 0xff, sizeof(int) * k, s);
+    cudaMemsetAsync(F.piv_rows, 0, sizeof(int) * k, s);   // in range even where a singular panel stops early
     cudaMemsetAsync(F.err, 0, sizeof(int), s);
     const bool smem = k <= GJ_SMEM_ROWS;
     const size_t psh = smem ? (size_t)k * GJ_NB * sizeof(double) + (size_t)k : 0;
@@ -223,14 +226,25 @@ cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s
         const int w = (k - c0 < GJ_NB) ? (k - c0) : GJ_NB;
         if (smem) k_gj_panel<512, true><<<1, 512, psh, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
         else k_gj_panel<512, false><<<1, 512, 0, s>>>(F.S, k, c0, w, F.Pan, F.Wk, F.rowpiv, F.piv_rows, F.Winv, F.err);
-        k_gj_rows<<<(k * GJ_NB + 255) / 256, 256, 0, s>>>(F.S, k, c0, w, F.piv_rows, F.Winv);
+        k_gj_rows<<<(k * GJ_NB + 255) / 256, 256, 0, s>>>(F.S, k, c0, w, F.piv_rows, F.Winv, F.err);
         dim3 g((k + 31) / 32, (k + 31) / 32), b(32, 32);
-        k_gj_update<<<g, b, 0, s>>>(F.S, k, c0, w, F.Pan, F.rowpiv, F.piv_rows, F.Winv);
+        k_gj_update<<<g, b, 0, s>>>(F.S, k, c0, w, F.Pan, F.rowpiv, F.piv_rows, F.Winv, F.err);
     }
     dim3 g((k + 31) / 32, (k + 31) / 32), b(32, 32);
-    k_gj_permute<<<g, b, 0, s>>>(F.S, k, F.piv_rows, D.Kinv);
-    count_launch(3 + 3 * ((k + GJ_NB - 1) / GJ_NB));
+    k_gj_permute<<<g, b, 0, s>>>(F.S, k, F.piv_rows, out, F.err);
+    count_launch(1 + 3 * ((k + GJ_NB - 1) / GJ_NB));
     return cudaGetLastError();
+}
+
+cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s) {
+    if (k == 0) return cudaSuccess;
+    const size_t kk = (size_t)k * k;
+    k_fill_zero<<<1184, 256, 0, s>>>(F.S, kk);
+    k_build_K<<<(k + 255) / 256, 256, 0, s>>>(D.cptr, D.crow, D.cval, F.s_var, F.row_kidx, k, F.S);
+    count_launch(2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return gj_inverse(F, k, D.Kinv, s);
 }
 
 }  // namespace ds

@@ -729,6 +729,89 @@ __global__ void k_btran_gemv(Dev D, double* out, int force) {
     }
 }
 
+// ============================================= sparse factor solves
+// B0 solves through the sparse LU of the bump (sparse_factor.cu): a program of
+// levels over one vector of k slots, in shared memory when it fits.  The ops
+// of a level are independent (the program builder puts every op above the ops
+// it reads), so one barrier per level orders them.
+constexpr int SF_BS = 1024;
+
+template <int BS>
+__device__ void sf_run(const SfDev& F, const SfProg& P, double* v, double* tmp) {
+    for (int L = 0; L < P.nlev; ++L) {
+        const int kind = P.lvl_kind[L];
+        if (kind == 0) {
+            const int o1 = P.lvl_ptr[L + 1];
+            for (int o = P.lvl_ptr[L] + threadIdx.x; o < o1; o += BS) {
+                const int s = P.op_slot[o];
+                double acc = v[s];
+                const int e1 = P.op_ptr[o + 1];
+                for (int e = P.op_ptr[o]; e < e1; ++e) acc -= P.ent_coef[e] * v[P.ent_slot[e]];
+                v[s] = acc / P.op_diag[o];
+            }
+        } else {   // dense block: v[d0 + o] = sum_i M[o + i kd] v[d0 + i]
+            const double* M = (kind == 1) ? F.Sinv : F.SinvT;
+            const int kd = F.kd, d0 = F.d0;
+            for (int o = threadIdx.x; o < kd; o += BS) {
+                double acc = 0.0;
+                for (int i = 0; i < kd; ++i) acc += M[o + (size_t)i * kd] * v[d0 + i];
+                tmp[o] = acc;
+            }
+            __syncthreads();
+            for (int o = threadIdx.x; o < kd; o += BS) v[d0 + o] = tmp[o];
+        }
+        __syncthreads();
+    }
+}
+
+// FTRAN through B0's bump for the nr right-hand sides (one CTA each): slot s
+// starts as the rhs entry of its pivot row and ends as the solution entry of
+// its pivot column, written to y0 at that column's basis position.
+template <int BS>
+__global__ void __launch_bounds__(BS) k_sf_ftran(Dev D, int nr_fixed, int force) {
+    pdl_enter();
+    Ctl* c = D.ctl;
+    if (!force && halted(c)) return;
+    const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
+    const int r = blockIdx.x;
+    if (r >= nr) return;
+    extern __shared__ double sf_vec[];
+    const SfDev& F = D.sf;
+    double* v = F.smem ? sf_vec : F.gvec + (size_t)r * F.k;
+    double* tmp = F.gtmp + (size_t)r * (F.kd > 0 ? F.kd : 1);
+    const double* rhs = D.frhs[r];
+    for (int s = threadIdx.x; s < F.k; s += BS) v[s] = rhs[F.slot_row[s]];
+    __syncthreads();
+    sf_run<BS>(F, F.ft, v, tmp);
+    double* y0 = D.y0[r];
+    for (int s = threadIdx.x; s < F.k; s += BS) y0[F.slot_pos[s]] = v[s];
+}
+
+// BTRAN through B0's bump (block 0: rho at the rows of R' from btr_rhs) and
+// the basis's slack rows (the other blocks: rho[r] = y[slackpos(r)]).
+template <int BS>
+__global__ void __launch_bounds__(BS) k_sf_btran(Dev D, double* out, int force) {
+    pdl_enter();
+    if (!force && halted(D.ctl)) return;
+    if (blockIdx.x == 0) {
+        extern __shared__ double sf_vec[];
+        const SfDev& F = D.sf;
+        double* v = F.smem ? sf_vec : F.gvec;
+        for (int s = threadIdx.x; s < F.k; s += BS) v[s] = D.btr_rhs[F.slot_kcol[s]];
+        __syncthreads();
+        sf_run<BS>(F, F.bt, v, F.gtmp);
+        for (int s = threadIdx.x; s < F.k; s += BS) out[F.slot_row[s]] = v[s];
+    } else {
+        const int r = (blockIdx.x - 1) * BS + threadIdx.x;
+        if (r >= D.m) return;
+        const int sp = D.row_slackpos[r];
+        if (sp >= 0) out[r] = D.ybt[sp];
+    }
+}
+
+static size_t sf_smem(const Dev& D) { return D.sf.smem ? sizeof(double) * (size_t)D.sf.k : 0; }
+static int sf_btran_blocks(const Dev& D) { return 1 + (D.m + SF_BS - 1) / SF_BS; }
+
 // ================================================================ pivot row
 // Full sequential ratio scan over F in slot order (simpleRatioTest, tpp:546-572):
 // the fallback when the tie window could not be shown exact.
@@ -1772,15 +1855,21 @@ cudaError_t launch_count_dual_inf(const Dev& D, cudaStream_t s) {
 
 cudaError_t launch_btran_b0(const Dev& D, double* out, int force, cudaStream_t s) {
     if (D.k > 0) k_btran_rhs<BS><<<nblk(D.k), BS, 0, s>>>(D, force);
-    const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
-    k_btran_gemv<BS><<<nbw + nblk(D.m), BS, 0, s>>>(D, out, force);
+    if (D.sf.on && D.k > 0) {
+        k_sf_btran<SF_BS><<<sf_btran_blocks(D), SF_BS, sf_smem(D), s>>>(D, out, force);
+    } else {
+        const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
+        k_btran_gemv<BS><<<nbw + nblk(D.m), BS, 0, s>>>(D, out, force);
+    }
     count_launch((D.k > 0 ? 1 : 0) + 1);
     LAUNCH_OK();
     return cudaSuccess;
 }
 
 cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaStream_t s) {
-    if (D.k > 0) {
+    if (D.k > 0 && D.sf.on) {
+        k_sf_ftran<SF_BS><<<MAX_FTRAN_RHS, SF_BS, sf_smem(D), s>>>(D, nr_fixed, force);
+    } else if (D.k > 0) {
         dim3 g(D.ftr_ntile, D.ftr_nchunk);
         const size_t sh = (size_t)D.ftr_chunk * MAX_FTRAN_RHS * sizeof(double);
         k_ftran_k2<BS><<<g, BS, sh, s>>>(D, nr_fixed, force);
@@ -1830,6 +1919,9 @@ static cudaError_t set_kernel_attributes(int cap) {
     if ((e = cudaFuncSetAttribute(k_btran_unit<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_ftran_assemble<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
     if ((e = cudaFuncSetAttribute(k_btran_dense_fix<BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess) return e;
+    const int sf_bytes = (int)(sizeof(double) * SF_SMEM_SLOTS);
+    if ((e = cudaFuncSetAttribute(k_sf_ftran<SF_BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sf_bytes)) != cudaSuccess) return e;
+    if ((e = cudaFuncSetAttribute(k_sf_btran<SF_BS>, cudaFuncAttributeMaxDynamicSharedMemorySize, sf_bytes)) != cudaSuccess) return e;
     // a 16-CTA cluster is above the portable size of 8
     if ((e = cudaFuncSetAttribute(k_dual_update_cluster<DU_BS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1)) != cudaSuccess)
         return e;
@@ -1904,8 +1996,13 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
             break;
         case S_BTRAN_RHS: { cudaError_t e = launch_pdl(k_btran_rhs<BS>, dim3(nblk(D.k)), dim3(BS), 0, s, D, 0); if (e) return e; break; }
         case S_BTRAN_GEMV: {
-            const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
-            cudaError_t e = launch_pdl(k_btran_gemv<BS>, dim3(nbw + nblk(D.m)), dim3(BS), 0, s, D, D.rho, 0);
+            cudaError_t e;
+            if (D.sf.on && D.k > 0) {
+                e = launch_pdl(k_sf_btran<SF_BS>, dim3(sf_btran_blocks(D)), dim3(SF_BS), sf_smem(D), s, D, D.rho, 0);
+            } else {
+                const int nbw = (D.k + BS / 32 - 1) / (BS / 32);
+                e = launch_pdl(k_btran_gemv<BS>, dim3(nbw + nblk(D.m)), dim3(BS), 0, s, D, D.rho, 0);
+            }
             if (e) return e;
             break;
         }
@@ -1922,7 +2019,10 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
             break;
         }
         case S_FTRAN_K:
-            if (D.k > 0) {
+            if (D.k > 0 && D.sf.on) {
+                cudaError_t e = launch_pdl(k_sf_ftran<SF_BS>, dim3(MAX_FTRAN_RHS), dim3(SF_BS), sf_smem(D), s, D, 0, 0);
+                if (e) return e;
+            } else if (D.k > 0) {
                 dim3 g(D.ftr_ntile, D.ftr_nchunk);
                 const size_t sh = (size_t)D.ftr_chunk * MAX_FTRAN_RHS * sizeof(double);
                 cudaError_t e = launch_pdl(k_ftran_k2<BS>, g, dim3(BS), sh, s, D, 0, 0);

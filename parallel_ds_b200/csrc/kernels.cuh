@@ -19,6 +19,8 @@ struct FactorBufs {
 };
 
 cudaError_t factor_bump(const FactorBufs& F, const Dev& D, int k, cudaStream_t s);
+// Gauss-Jordan inverse of the k x k column-major matrix already in F.S, written to out.
+cudaError_t gj_inverse(const FactorBufs& F, int k, double* out, cudaStream_t s);
 
 // Kernels of one iteration, in launch order.
 // PFI mode runs S_BTRAN_RHS .. S_ETA_APPLY; dense mode runs S_FTRAN_DENSE and S_BINV

@@ -196,7 +196,7 @@ class CudaDualSimplex:
     def __init__(self, problem, refactor_interval=100, max_iterations=2000000, pricing="dse",
                  strict_reference=False, seed=12345, device=0, learned_margin=0.5, learned_mix=0.05,
                  learned_pdhg_iters=4000, dense_max_m=4096, dense_refactor_interval=400,
-                 learned_start_iteration=-1, pdhg_cluster=1, model=None, verbose=0):
+                 learned_start_iteration=-1, pdhg_cluster=1, model=None, verbose=0, factor="sparse"):
         self.problem = problem
         self.L = _lib.lib()
         o = DsOptions()
@@ -214,6 +214,9 @@ class CudaDualSimplex:
         o.dense_refactor_interval = dense_refactor_interval
         o.learned_start_iteration = learned_start_iteration
         o.pdhg_cluster = pdhg_cluster
+        if factor not in ("sparse", "dense"):
+            raise ValueError(f"unknown factorisation {factor!r}")
+        o.factor_mode = _lib.FACTOR_DENSE if factor == "dense" else _lib.FACTOR_SPARSE
         o.verbose = verbose
         self.opts = o
         self.h = C.c_void_p()
