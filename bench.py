@@ -318,6 +318,137 @@ def our_arm(args, rank, world, local_rank):
     return res
 
 
+def large_arm(args, rank, world, local_rank):
+    """The large eta-file workload (m=50,000, n=100,000, 8 nonzeros per column):
+    one step = the first --large-iters iterations of a plain DSE solve of one
+    seeded LP from its slack basis (refactorisations every 100 iterations by
+    the sparse LU included), LP resident in HBM.  Metric: iterations/s."""
+    import numpy as np
+    import torch
+    from parallel_ds_b200 import _lib
+    from parallel_ds_b200 import lp as L
+    from parallel_ds_b200._lib import DsOptions, DsStats, ptr
+
+    torch.cuda.set_device(local_rank)
+    lib = _lib.lib()
+    cap = args.large_iters
+
+    def new_handle():
+        h = C.c_void_p()
+        o = DsOptions()
+        lib.ds_default_options(C.byref(o))
+        o.device = local_rank
+        o.max_iterations = cap
+        assert lib.ds_create(C.byref(o), C.byref(h)) == 0
+        return h
+
+    def load(h, t):
+        rc = lib.ds_load_typed(h, t["m"], t["n"], ptr(t["row_ptr"], C.c_int), ptr(t["col_idx"], C.c_int),
+                               ptr(t["val"], C.c_double), ptr(t["c"], C.c_double), ptr(t["col_type"], C.c_int),
+                               ptr(t["col_lb"], C.c_double), ptr(t["col_ub"], C.c_double),
+                               ptr(t["row_type"], C.c_int), ptr(t["row_lb"], C.c_double),
+                               ptr(t["row_ub"], C.c_double))
+        assert rc == 0, lib.ds_last_error(h)
+
+    def stats(h):
+        st = DsStats()
+        lib.ds_get_stats(h, C.byref(st))
+        return st
+
+    K, W = args.steps, args.warmup
+    seeds = [2000 + rank * K + s for s in range(K)]
+    lps = [pinned_copy(L.typed(gen(args.workload, x))) for x in seeds]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    hw = new_handle()
+    for s in range(W):
+        load(hw, L.typed(gen(args.workload, 1000 + rank * W + s)))
+        assert lib.ds_solve(hw) == 0, lib.ds_last_error(hw)
+    hs = [new_handle() for _ in lps]
+    for h, t in zip(hs, lps):
+        load(h, t)
+    torch.cuda.synchronize()
+    clk = Clocks(local_rank) if rank == 0 else None
+    if clk:
+        clk.start(); time.sleep(0.6)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = lib.ds_kernel_launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for s, h in enumerate(hs):
+        flush.fill_(float(s))
+        ev[s][0].record()
+        assert lib.ds_solve(h) == 0, lib.ds_last_error(h)
+        ev[s][1].record()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = lib.ds_kernel_launch_count() - launches0
+    clocks = clk.stop() if clk else None
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    iters = sum(stats(h).iterations for h in hs)
+    refac_ms = sum(stats(h).refactor_ms for h in hs)
+    st0 = stats(hs[0])
+    # e2e: load from pinned host buffers, solve, read x and y back
+    x, y = np.zeros(lps[0]["n"]), np.zeros(lps[0]["m"])
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    e_it = 0
+    for t in lps:
+        load(hw, t)
+        assert lib.ds_solve(hw) == 0, lib.ds_last_error(hw)
+        lib.ds_get_primal(hw, ptr(x, C.c_double), None)
+        lib.ds_get_dual(hw, ptr(y, C.c_double))
+        e_it += stats(hw).iterations
+    torch.cuda.synchronize()
+    e_ms = (time.perf_counter() - e0) * 1e3
+    roof = profile_roofline(lib, hs[0])
+    for h in hs + [hw]:
+        lib.ds_destroy(h)
+    if world > 1:
+        tt = torch.tensor([t_ms, e_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        it = torch.tensor([iters, e_it], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(it, op=torch.distributed.ReduceOp.SUM)
+        t_ms, e_ms = [float(v) for v in tt.tolist()]
+        iters, e_it = [int(v) for v in it.tolist()]
+    if rank != 0:
+        return None
+    res = {
+        "metric": "iterations/s of the plain GPU dual simplex (eta file + sparse LU), first %d iterations" % cap,
+        "value": iters / (t_ms / 1e3), "unit": "iterations/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": t_ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: seeded generator, 8 N(0,1) entries per column at uniform random rows",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": "dse", "iterations_per_step": cap,
+                   "refactor_interval": 100, "seeds_rank0": f"{seeds[0]}..{seeds[-1]}",
+                   "l2": "256 MB buffer written between steps (flush)",
+                   "step": f"one LP, its first {cap} iterations from the slack basis"},
+        "refactor_ms_per_step": refac_ms / K,
+        "last_factor": {"bump": st0.bump_size, "kernel": st0.lu_kernel, "dense_block": st0.lu_dense,
+                        "levels_ftran_btran": st0.lu_levels, "markowitz_rounds": st0.lu_rounds},
+        "e2e": {"value": e_it / (e_ms / 1e3), "unit": "iterations/s",
+                "h2d_bytes_per_step": int(lp_bytes(lps[0])),
+                "d2h_bytes_per_step": int(8 * (lps[0]["n"] + lps[0]["m"])), "ms_per_step": e_ms / K},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if roof:
+        res["roofline"] = roof
+    return res
+
+
+def large_cpu_sample(workload, iters=300):
+    """The oracle running the first `iters` iterations of the same LP on one core."""
+    from oracle import pyoracle as po
+    from parallel_ds_b200 import lp as L
+    t = L.typed(gen(workload, 2000))
+    t0 = time.perf_counter()
+    r = po.solve_typed(t, max_iterations=iters)
+    dt = time.perf_counter() - t0
+    return {"value": r["iterations"] / dt, "unit": "iterations/s", "cores": 1, "kind": "port",
+            "sample": f"oracle runs the first {r['iterations']} iterations of seed 2000 ({r['status']}), {dt:.1f} s"}
+
+
 def batch_arm(args, rank, world, local_rank):
     """Batched workloads: one step = one persistent launch solving the whole
     batch (`count` LPs per GPU, weak scaling: rank r solves seeds
@@ -586,6 +717,8 @@ def main():
     ap.add_argument("--no-pdhg-cluster", action="store_true", help="PDHG on the launch-per-step graph path")
     ap.add_argument("--no-tune", action="store_true", help="batched workloads: default schedule, no autotuning")
     ap.add_argument("--max-iterations", type=int, default=0, help="--solve-one: iteration cap (0: none)")
+    ap.add_argument("--large-iters", type=int, default=3000,
+                    help="plain_large workload: iterations of each step's solve (iteration cap)")
     ap.add_argument("--batch-count", type=int, default=0,
                     help="batched workloads: LPs per GPU (default: the workload's 4096 / 65,536)")
     args = ap.parse_args()
@@ -614,10 +747,12 @@ def main():
         import torch
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    res = (batch_arm if args.workload in BATCH else our_arm)(args, rank, world, local_rank)
+    arm = batch_arm if args.workload in BATCH else (large_arm if args.workload == "plain_large" else our_arm)
+    res = arm(args, rank, world, local_rank)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             res["cpu_baseline"] = (batch_cpu_sample(args.workload) if args.workload in BATCH
+                                   else large_cpu_sample(args.workload) if args.workload == "plain_large"
                                    else cpu_sample(args.workload))
         print(json.dumps(res))
     if world > 1:

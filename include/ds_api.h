@@ -330,6 +330,14 @@ int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, const double
 int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos,
                         const double* rhs, double* sol, int transpose);
 
+/* Device time in milliseconds (CUDA events on the default stream) of the
+ * kernels that the calling thread's last ds_kernel_pivot_row or
+ * ds_kernel_pfi_apply call launched, host copies excluded: the per-kernel
+ * figure compared with the reference's spmvUpdateTKernel and etaSolveKernel
+ * (cudaKernels.cu:108-157, 266-322) on identical inputs.  No reference
+ * counterpart.  DS_ERR_STATE if no timed call ran yet. */
+int ds_kernel_last_time(double* ms);
+
 /* ---- batched persistent solver -------------------------------------------------
  * No counterpart in the reference.  Many independent LPs
  *     min c^T x  s.t.  A x <= b,  x >= 0        (m <= DS_BATCH_MAX_M, any n)

@@ -104,6 +104,7 @@ def lib():
         "ds_kernel_ratio_test": (C.c_int, [C.c_int, C.c_int, IP, DP, C.c_double, C.c_int, DP, DP, DP, DP,
                                            IP, IP, IP, DP, DP, IP]),
         "ds_kernel_pfi_apply": (C.c_int, [C.c_int, C.c_int, DP, IP, DP, DP, C.c_int]),
+        "ds_kernel_last_time": (C.c_int, [DP]),
         "ds_kernel_ratio_test_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                    IP, IP, DP, DP, IP, C.c_void_p]),

@@ -73,7 +73,12 @@ def build(verbose=False):
 
 
 def build_oracle():
-    return _run(["make", "-C", os.path.join(ROOT, "oracle")])
+    out = _run(["make", "-C", os.path.join(ROOT, "oracle")])
+    ref = os.environ.get("DS_REFERENCE_ROOT", "/root/reference")
+    if os.path.exists(os.path.join(ref, "src", "gpu", "cudaKernels.cu")):
+        # the reference's own kernels, the same-box per-kernel baseline (oracle/_ref)
+        out += _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "REF=" + ref])
+    return out
 
 
 if __name__ == "__main__":

@@ -50,6 +50,20 @@ std::vector<unsigned char> types_u8(const int* t, int n) {
     return v;
 }
 
+// Device time of the kernels the last timed ds_kernel_* call launched (this thread).
+thread_local double g_last_ms = -1.0;
+
+struct KernelTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    KernelTimer() { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, 0); }
+    void stop() {
+        cudaEventRecord(b, 0);
+        float ms = -1.0f;
+        if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess) g_last_ms = ms;
+    }
+    ~KernelTimer() { if (a) cudaEventDestroy(a); if (b) cudaEventDestroy(b); }
+};
+
 int finish(cudaError_t e) {
     if (e != cudaSuccess) return DS_ERR_CUDA;
     e = cudaDeviceSynchronize();
@@ -102,7 +116,11 @@ int ds_kernel_pivot_row(int m, int n, const int* csc_ptr, const int* csc_row, co
     D.alpha = s.alloc<double>(n);
     D.redi = s.alloc<int>(n / 256 + 8);
     D.ctl = new_ctl(s);
-    int rc = finish(launch_pivot_row_mode(D, 1, 0));
+    cudaDeviceSynchronize();
+    KernelTimer tm;
+    cudaError_t le = launch_pivot_row_mode(D, 1, 0);
+    tm.stop();
+    int rc = finish(le);
     if (rc) return rc;
     cudaMemcpy(alpha, D.alpha, sizeof(double) * n, cudaMemcpyDeviceToHost);
     return DS_OK;
@@ -166,7 +184,9 @@ int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos, const d
     D.y0[0] = d_y0; D.frhs[0] = d_rhs; D.fout[0] = d_out;
     D.ctl = new_ctl(s);
     if (init_kernel_attributes(D.cap) != cudaSuccess) return DS_ERR_CUDA;
-    cudaError_t e = launch_build_mtri(D, T, 0);
+    cudaError_t e = launch_build_mtri(D, T, 0);   // the eta file's G, kept between iterations by the engine
+    cudaDeviceSynchronize();
+    KernelTimer tm;
     if (e == cudaSuccess) {
         if (!transpose) e = launch_ftran(D, 1, 0, 1, 0);
         else {
@@ -174,10 +194,17 @@ int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos, const d
             if (e == cudaSuccess) e = launch_btran_b0(D, d_out, 1, 0);
         }
     }
+    tm.stop();
     int rc = finish(e);
     if (rc) return rc;
     cudaMemcpy(sol, d_out, sizeof(double) * m, cudaMemcpyDeviceToHost);
     return DS_OK;
+}
+
+int ds_kernel_last_time(double* ms) {
+    if (!ms) return DS_ERR_ARG;
+    *ms = g_last_ms;
+    return g_last_ms >= 0.0 ? DS_OK : DS_ERR_STATE;
 }
 
 }  // extern "C"

@@ -240,24 +240,52 @@ __device__ void stage_G(const Dev& D, double* Gs, int T) {
     for (int t = 1; t < T; ++t)
         if (u < t) Gs[pk(t, u)] = __ldcg(&D.Mtri[(size_t)t * D.cap + u]);
 }
+// The chain recurrences, one warp, in blocks of 32 unknowns: each lane owns one
+// unknown of the block, first sums the contributions of the blocks already
+// solved (its own dot product, no shuffles), then the block's triangle is
+// walked one unknown at a time, the finished value broadcast by a shuffle and
+// folded into the lanes still open.  T sequential steps of a shuffle and a
+// fused update instead of T warp-wide reductions.
 __device__ void eta_forward(const double* Gs, const double* g, double* s, int T) {
     const int lane = threadIdx.x & 31;
-    for (int t = 0; t < T; ++t) {
-        const double* Gr = Gs + pk(t, 0);
+    for (int b0 = 0; b0 < T; b0 += 32) {
+        const int t = b0 + lane;
         double v = 0.0;
-        for (int u = lane; u < t; u += 32) v += Gr[u] * s[u];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) s[t] = g[t] + v;
+        if (t < T) {
+            const double* Gr = Gs + pk(t, 0);
+            double a0 = 0.0, a1 = 0.0;
+            int u = 0;
+            for (; u + 1 < b0; u += 2) { a0 += Gr[u] * s[u]; a1 += Gr[u + 1] * s[u + 1]; }
+            if (u < b0) a0 += Gr[u] * s[u];
+            v = g[t] + (a0 + a1);
+        }
+        const int nb = min(32, T - b0);
+        for (int j = 0; j < nb; ++j) {
+            const double sj = __shfl_sync(0xffffffffu, v, j);
+            if (lane > j && t < T) v += Gs[pk(t, b0 + j)] * sj;
+        }
+        if (t < T) s[t] = v;
         __syncwarp();
     }
 }
 __device__ void eta_backward(const double* Gs, const double* h, double* dl, int T) {
     const int lane = threadIdx.x & 31;
-    for (int t = T - 1; t >= 0; --t) {
+    for (int b1 = T - 1; b1 >= 0; b1 -= 32) {
+        const int t = b1 - lane;
         double v = 0.0;
-        for (int u = t + 1 + lane; u < T; u += 32) v += Gs[pk(u, t)] * dl[u];
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if (lane == 0) dl[t] = h[t] + v;
+        if (t >= 0) {
+            double a0 = 0.0, a1 = 0.0;
+            int u = b1 + 1;
+            for (; u + 1 < T; u += 2) { a0 += Gs[pk(u, t)] * dl[u]; a1 += Gs[pk(u + 1, t)] * dl[u + 1]; }
+            if (u < T) a0 += Gs[pk(u, t)] * dl[u];
+            v = h[t] + (a0 + a1);
+        }
+        const int nb = min(32, b1 + 1);
+        for (int j = 0; j < nb; ++j) {
+            const double dj = __shfl_sync(0xffffffffu, v, j);
+            if (lane > j && t >= 0) v += Gs[pk(b1 - j, t)] * dj;
+        }
+        if (t >= 0) dl[t] = v;
         __syncwarp();
     }
 }
@@ -1319,44 +1347,59 @@ __global__ void k_ftran_assemble(Dev D, int nr_fixed, int force) {
         for (int q = 0; q < nr; ++q) D.s_eta[q * D.cap + t] = sv[q][t];
 }
 
-// y = y0 + sum_t s_t eta_t, streaming over the eta file (64-thread blocks so
-// that small m still spreads over many SMs); the last block applies the
-// -s_t e_{p_t} terms (duplicated positions summed in eta order by the thread
-// owning the first occurrence) and, for the iteration FTRAN, the pivot check
+// y = y0 + sum_t s_t eta_t, streaming over the eta file: a block covers ROWS
+// rows with ETA_SPLIT thread groups, group g summing its contiguous share of
+// the etas (more loads in flight per row than one thread could keep), the
+// partials added in group order.  The last block applies the -s_t e_{p_t}
+// terms (duplicated positions summed in eta order by the thread owning the
+// first occurrence) and, for the iteration FTRAN, the pivot check
 // |alpha_q[p] - alpha_p[q]| > EPS_R (1 + |alpha_q[p]|)  (cudaDualSimplex.cpp:555).
-template <int BS>
-__global__ void k_eta_apply(Dev D, int nr_fixed, int check, int force) {
+constexpr int ETA_SPLIT = 4;
+template <int ROWS>
+__global__ void __launch_bounds__(ROWS * ETA_SPLIT) k_eta_apply(Dev D, int nr_fixed, int check, int force) {
+    constexpr int BS = ROWS * ETA_SPLIT;
     pdl_enter();
     Ctl* c = D.ctl;
     if (!force && halted(c)) return;
     const int nr = nr_fixed > 0 ? nr_fixed : c->nrhs;
     const int T = c->T;
-    const int i = blockIdx.x * BS + threadIdx.x;
+    const int r = threadIdx.x % ROWS, g = threadIdx.x / ROWS;
+    const int i = blockIdx.x * ROWS + r;
     __shared__ double s[MAX_FTRAN_RHS][256];
+    __shared__ double part[ETA_SPLIT][MAX_FTRAN_RHS][ROWS];
     for (int q = 0; q < nr; ++q)
         for (int t = threadIdx.x; t < T; t += BS) s[q][t] = D.s_eta[q * D.cap + t];
     __syncthreads();
+    const int chunk = (T + ETA_SPLIT - 1) / ETA_SPLIT;
+    const int t0 = g * chunk, t1 = min(T, t0 + chunk);
     if (i < D.m) {
         const double* e = D.eta + i;
         const size_t M = D.m;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
         if (nr == 1) {
-            double a0 = D.y0[0][i], b0 = 0.0;
-            int t = 0;
-            for (; t + 1 < T; t += 2) { a0 += s[0][t] * e[t * M]; b0 += s[0][t + 1] * e[(t + 1) * M]; }
-            if (t < T) a0 += s[0][t] * e[t * M];
-            D.fout[0][i] = a0 + b0;
+            double b0 = 0.0;
+            int t = t0;
+#pragma unroll 4
+            for (; t + 1 < t1; t += 2) { a0 += s[0][t] * e[t * M]; b0 += s[0][t + 1] * e[(t + 1) * M]; }
+            if (t < t1) a0 += s[0][t] * e[t * M];
+            a0 += b0;
         } else {
-            double a0 = D.y0[0][i], a1 = D.y0[1][i], a2 = (nr > 2) ? D.y0[2][i] : 0.0;
 #pragma unroll 8
-            for (int t = 0; t < T; ++t) {
+            for (int t = t0; t < t1; ++t) {
                 const double ev = e[t * M];
                 a0 += s[0][t] * ev;
                 a1 += s[1][t] * ev;
                 if (nr > 2) a2 += s[2][t] * ev;
             }
-            D.fout[0][i] = a0;
-            D.fout[1][i] = a1;
-            if (nr > 2) D.fout[2][i] = a2;
+        }
+        part[g][0][r] = a0; part[g][1][r] = a1; part[g][2][r] = a2;
+    }
+    __syncthreads();
+    if (g == 0 && i < D.m) {
+        for (int q = 0; q < nr; ++q) {
+            double acc = D.y0[q][i];
+            for (int gg = 0; gg < ETA_SPLIT; ++gg) acc += part[gg][q][r];
+            D.fout[q][i] = acc;
         }
     }
     if (!last_block(&c->tickets[6])) return;
@@ -1875,7 +1918,7 @@ cudaError_t launch_ftran(const Dev& D, int nr_fixed, int check, int force, cudaS
         k_ftran_k2<BS><<<g, BS, sh, s>>>(D, nr_fixed, force);
     }
     k_ftran_assemble<BS><<<nblk(D.m), BS, g_smem_bytes(D.cap), s>>>(D, nr_fixed, force);
-    k_eta_apply<BS_ETA><<<(D.m + BS_ETA - 1) / BS_ETA, BS_ETA, 0, s>>>(D, nr_fixed, check, force);
+    k_eta_apply<BS_ETA><<<(D.m + BS_ETA - 1) / BS_ETA, BS_ETA * ETA_SPLIT, 0, s>>>(D, nr_fixed, check, force);
     count_launch((D.k > 0 ? 1 : 0) + 2);
     LAUNCH_OK();
     return cudaSuccess;
@@ -2032,7 +2075,7 @@ cudaError_t launch_step(const Dev& D, int step, cudaStream_t s) {
             }
             break;
         case S_FTRAN_ASM: { cudaError_t e = launch_pdl(k_ftran_assemble<BS>, dim3(nblk(D.m)), dim3(BS), g_smem_bytes(D.cap), s, D, 0, 0); if (e) return e; break; }
-        case S_ETA_APPLY: { cudaError_t e = launch_pdl(k_eta_apply<BS_ETA>, dim3((D.m + BS_ETA - 1) / BS_ETA), dim3(BS_ETA), 0, s, D, 0, 1, 0); if (e) return e; break; }
+        case S_ETA_APPLY: { cudaError_t e = launch_pdl(k_eta_apply<BS_ETA>, dim3((D.m + BS_ETA - 1) / BS_ETA), dim3(BS_ETA * ETA_SPLIT), 0, s, D, 0, 1, 0); if (e) return e; break; }
         case S_UPDATE: { cudaError_t e = launch_pdl(k_update<BS>, dim3(nblk(D.m)), dim3(BS), 0, s, D, 0); if (e) return e; break; }
         default: return cudaErrorInvalidValue;
     }
