@@ -764,18 +764,52 @@ __global__ void k_btran_gemv(Dev D, double* out, int force) {
 // it reads), so one barrier per level orders them.
 constexpr int SF_BS = 1024;
 
+// One op's program data: its slot, divisor, entry range and first entries.
+// The data of a thread's first op of the next level is loaded before the
+// level barrier (it does not depend on the vector), so each level pays only
+// the barrier and the shared-memory arithmetic, not a chain of L2 loads.
+constexpr int SF_PRE = 4;
+constexpr int SF_MAXLEV = 512;   // level bounds staged in shared memory up to this many levels
+struct SfOp { int s, e0, e1; double dg; int es[SF_PRE]; double cf[SF_PRE]; };
+__device__ __forceinline__ void sf_load_op(const SfProg& P, int o, SfOp& q) {
+    q.s = P.op_slot[o]; q.e0 = P.op_ptr[o]; q.e1 = P.op_ptr[o + 1]; q.dg = P.op_diag[o];
+#pragma unroll
+    for (int u = 0; u < SF_PRE; ++u) {
+        const bool in = q.e0 + u < q.e1;
+        q.es[u] = in ? P.ent_slot[q.e0 + u] : 0;
+        q.cf[u] = in ? P.ent_coef[q.e0 + u] : 0.0;
+    }
+}
+
 template <int BS>
-__device__ void sf_run(const SfDev& F, const SfProg& P, double* v, double* tmp) {
+__device__ __forceinline__ void sf_run(const SfDev& F, const SfProg& P, double* v, double* tmp) {
+    __shared__ int s_lp[SF_MAXLEV + 1];
+    __shared__ int s_lk[SF_MAXLEV];
+    const bool staged = P.nlev <= SF_MAXLEV;
+    if (staged) {
+        for (int L = threadIdx.x; L <= P.nlev; L += BS) s_lp[L] = P.lvl_ptr[L];
+        for (int L = threadIdx.x; L < P.nlev; L += BS) s_lk[L] = P.lvl_kind[L];
+    }
+    __syncthreads();
+    const int* lp = staged ? s_lp : P.lvl_ptr;
+    const int* lk = staged ? s_lk : P.lvl_kind;
+    SfOp q;
+    bool have = false;
+    if (P.nlev > 0 && lk[0] == 0 && lp[0] + (int)threadIdx.x < lp[1]) { sf_load_op(P, lp[0] + threadIdx.x, q); have = true; }
     for (int L = 0; L < P.nlev; ++L) {
-        const int kind = P.lvl_kind[L];
+        const int kind = lk[L];
         if (kind == 0) {
-            const int o1 = P.lvl_ptr[L + 1];
-            for (int o = P.lvl_ptr[L] + threadIdx.x; o < o1; o += BS) {
-                const int s = P.op_slot[o];
-                double acc = v[s];
-                const int e1 = P.op_ptr[o + 1];
-                for (int e = P.op_ptr[o]; e < e1; ++e) acc -= P.ent_coef[e] * v[P.ent_slot[e]];
-                v[s] = acc / P.op_diag[o];
+            const int o0 = lp[L] + threadIdx.x, o1 = lp[L + 1];
+            for (int o = o0; o < o1; o += BS) {
+                SfOp c;
+                if (o == o0 && have) c = q;
+                else sf_load_op(P, o, c);
+                double acc = v[c.s];
+#pragma unroll
+                for (int u = 0; u < SF_PRE; ++u)
+                    if (c.e0 + u < c.e1) acc -= c.cf[u] * v[c.es[u]];
+                for (int e = c.e0 + SF_PRE; e < c.e1; ++e) acc -= P.ent_coef[e] * v[P.ent_slot[e]];
+                v[c.s] = acc / c.dg;
             }
         } else {   // dense block: v[d0 + o] = sum_i M[o + i kd] v[d0 + i]
             const double* M = (kind == 1) ? F.Sinv : F.SinvT;
@@ -787,6 +821,11 @@ __device__ void sf_run(const SfDev& F, const SfProg& P, double* v, double* tmp) 
             }
             __syncthreads();
             for (int o = threadIdx.x; o < kd; o += BS) v[d0 + o] = tmp[o];
+        }
+        have = false;
+        if (L + 1 < P.nlev && lk[L + 1] == 0 && lp[L + 1] + (int)threadIdx.x < lp[L + 2]) {
+            sf_load_op(P, lp[L + 1] + threadIdx.x, q);
+            have = true;
         }
         __syncthreads();
     }

@@ -140,3 +140,24 @@ def test_load_rejects_bad_input():
         rc = bs.L.ds_batch_load(bs.h, 1, ptr(m, C.c_int), ptr(n, C.c_int), ptr(cp, C.c_int), ptr(ri, C.c_int),
                                 ptr(va, C.c_double), ptr(b, C.c_double), ptr(c, C.c_double))
         assert rc == -1                                        # DS_ERR_ARG
+
+
+@pytest.mark.parametrize("count,m_lo,m_hi,seed", [(4096, 32, 512, 7000), (65536, 16, 64, 9000)])
+def test_full_batched_workloads(count, m_lo, m_hi, seed):
+    """The two batched workloads at full size (4096 LPs with m ~ U{32..512};
+    65,536 LPs with m ~ U{16..64}; 10% density), autotuned and solved in one
+    persistent launch: every status optimal, and 64 instances drawn at random
+    checked against HiGHS (objective, primal and dual feasibility)."""
+    bs = BatchSolver()
+    bs.generate(count, m_lo, m_hi, 0.10, seed=seed)
+    bs.tune()
+    bs.solve()
+    st, obj, it = bs.results()
+    assert len(st) == count
+    assert np.all(st == 1), np.unique(st, return_counts=True)
+    assert it.min() >= 0 and it.mean() > 1     # a few small instances are optimal at the slack basis
+    pick = np.random.default_rng(seed).choice(count, size=64, replace=False)
+    for i in pick:
+        lp = L.batched_instance(seed, int(i), m_lo, m_hi, 0.10)
+        x, y = bs.solution(int(i))
+        check_instance(lp, st[i], obj[i], x, y)

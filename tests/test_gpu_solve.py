@@ -98,7 +98,7 @@ def test_plain_small_trajectory_matches_oracle():
     np.testing.assert_allclose(tr["theta"][:first_diff], orc["trace"]["theta"][:first_diff], rtol=1e-9, atol=1e-12)
 
 
-@pytest.mark.parametrize("seed", [0, 1])
+@pytest.mark.parametrize("seed", range(8))
 def test_learned_size_vs_highs(seed):
     lp = L.learned(seed)
     res = S.solve_lp(lp, **MODE)

@@ -47,3 +47,18 @@ def test_sparse_and_gauss_jordan_factors_agree():
     b = S.solve_lp(lp, dense_max_m=0, factor="dense")
     assert a["status"] == b["status"] == "optimal"
     assert abs(a["objective"] - b["objective"]) <= 1e-9 * max(1.0, abs(b["objective"]))
+
+
+@pytest.mark.parametrize("dense_max_m", [0, 4096])
+def test_block_angular_scaled_vs_highs(dense_max_m):
+    """The block-angular workload's structure at a scale the test suite can
+    afford: 8 diagonal blocks of 400 x 800 (4 nonzeros per block column, as
+    the 4000 x 8000 blocks at 0.1% have) plus 50 linking rows over all
+    columns at 0.5%; eta-file mode (sparse LU) and dense mode."""
+    lp = L.generate(_lib.GEN_BLOCK, 8 * 400 + 50, 8 * 800, blocks=8, block_m=400, block_n=800, link_rows=50,
+                    block_density=0.01, link_density=0.005, seed=4)
+    res = S.solve_lp(lp, dense_max_m=dense_max_m)
+    h = highs(lp)
+    assert res["status"] == "optimal"
+    assert abs(res["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun)), (res["objective"], h.fun)
+    assert feasibility(lp, res["x"][:lp["n"]]) <= 1e-7
