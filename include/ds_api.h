@@ -238,6 +238,15 @@ int ds_model_train(ds_model* m, const float* X, const float* y, int rows, int ep
 /* Attach a model (not owned; NULL detaches).  Required when pricing is
  * DS_PRICING_LEARNED; must live on the solver's device. */
 int ds_set_model(ds_solver* s, ds_model* m);
+/* Failure-path testing of the scorer's bounded waits.  No reference
+ * counterpart.  polls > 0 replaces the bound of the wait for the network's
+ * tensor-core MMAs by that many non-blocking polls (after which the kernel
+ * still waits, bounded, for the MMAs to finish before it reads or frees their
+ * TMEM columns): too short a bound makes the scoring launches time out, their
+ * scores unusable (DSE prices those iterations) and ds_solve return
+ * DS_ERR_DEVICE_WAIT with the solve otherwise complete.  polls = 0 restores the
+ * default bound (2^26 polls).  Also clears the model's timeout flag. */
+int ds_model_set_wait_limit(ds_model* m, int polls);
 /* PDHG estimate of an optimal primal-dual pair of the loaded LP after iters
  * iterations (rounded up to whole restart periods of 500): x (n), row duals
  * y (m) with c + A^T y the reduced costs.  The learned scorer's warm-start

@@ -91,6 +91,7 @@ def lib():
         "ds_set_feature_trace": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
         "ds_get_feature_trace": (C.c_int, [C.c_void_p, FP, IP, IP, IP]),
         "ds_set_model": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "ds_model_set_wait_limit": (C.c_int, [C.c_void_p, C.c_int]),
         "ds_pdhg_estimate": (C.c_int, [C.c_void_p, C.c_int, DP, DP]),
         "ds_model_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
         "ds_model_destroy": (C.c_int, [C.c_void_p]),

@@ -70,8 +70,31 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
 }
 
 // Bounded wait for mbarrier phase `parity`; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+// test_polls > 0 (set by ds_model_set_wait_limit for failure-path tests)
+// replaces the bound by that many non-blocking polls; when they run out, the
+// wait still drains (bounded) until the MMAs have finished, because they keep
+// writing their TMEM columns, which are then read and freed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, int test_polls) {
     const uint32_t addr = smem_u32(mbar);
+    if (test_polls > 0) {
+        for (int it = 0; it < test_polls; ++it) {
+            uint32_t done;
+            asm volatile("{\n\t.reg .pred P1;\n\t"
+                         "mbarrier.test_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                         "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                         : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+            if (done) return true;
+        }
+        for (long it = 0; it < (1L << 26); ++it) {
+            uint32_t done;
+            asm volatile("{\n\t.reg .pred P1;\n\t"
+                         "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                         "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                         : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+            if (done) break;
+        }
+        return false;
+    }
     for (long it = 0; it < (1L << 26); ++it) {
         uint32_t done;
         asm volatile("{\n\t.reg .pred P1;\n\t"
@@ -289,7 +312,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
         umma_bf16(tm, kmajor_desc(smem_u32(sA1)), kmajor_desc(smem_u32(sB1)), idesc_bf16(128, 64), 0u);
         umma_commit(&mbar);
     }
-    if (!mbar_wait(&mbar, 0)) bad = 1;
+    if (!mbar_wait(&mbar, 0, a.err ? a.err[1] : 0)) bad = 1;
     tc_after_sync();
     float h[64];
     tmem_ld64(tm + lane_base, h);
@@ -308,7 +331,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(FwdArgs a, Dev D, int mode) {
                       idesc_bf16(128, 64), s > 0 ? 1u : 0u);
         umma_commit(&mbar);
     }
-    if (!mbar_wait(&mbar, 1)) bad = 1;
+    if (!mbar_wait(&mbar, 1, a.err ? a.err[1] : 0)) bad = 1;
     tc_after_sync();
     tmem_ld64(tm + lane_base + 64, h);
     float logit = sP[192];
@@ -440,7 +463,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(BwdArgs a) {
         out[OFF_B3] = s;
         out[NPARAMS] = l;
     }
-    if (!mbar_wait(&mbar, 0)) bad = 1;
+    if (!mbar_wait(&mbar, 0, a.err ? a.err[1] : 0)) bad = 1;
     tc_after_sync();
     __syncthreads();                     // sF reads above are done
     float v[64];
@@ -466,7 +489,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(BwdArgs a) {
         for (int r = 0; r < 128; ++r) s += sF[r * 65 + tid];
         out[OFF_B1 + tid] = s;
     }
-    if (!mbar_wait(&mbar, 1)) bad = 1;
+    if (!mbar_wait(&mbar, 1, a.err ? a.err[1] : 0)) bad = 1;
     tc_after_sync();
     // dW2[o][i] = dW2^T[i][o]: rows i = 0..63 sit in TMEM lanes 0..63 (warps 0, 1)
     if (warp < 2) {
@@ -662,11 +685,11 @@ int ds_model_create(int device, ds_model** out) {
     ok = ok && cudaMalloc(&md->loss, sizeof(float)) == cudaSuccess;
     ok = ok && cudaMalloc(&md->W1b, 64 * 16 * sizeof(__nv_bfloat16)) == cudaSuccess;
     ok = ok && cudaMalloc(&md->W2b, 64 * 64 * sizeof(__nv_bfloat16)) == cudaSuccess;
-    ok = ok && cudaMalloc(&md->err, sizeof(int)) == cudaSuccess;
+    ok = ok && cudaMalloc(&md->err, 2 * sizeof(int)) == cudaSuccess;   // [0] timeout flag, [1] test poll bound
     ok = ok && cudaMemsetAsync(md->P, 0, ds::NPARAMS * sizeof(float), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->m1, 0, ds::NPARAMS * sizeof(float), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->m2, 0, ds::NPARAMS * sizeof(float), md->stream) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(md->err, 0, sizeof(int), md->stream) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(md->err, 0, 2 * sizeof(int), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->W1b, 0, 64 * 16 * sizeof(__nv_bfloat16), md->stream) == cudaSuccess;
     ok = ok && cudaMemsetAsync(md->W2b, 0, 64 * 64 * sizeof(__nv_bfloat16), md->stream) == cudaSuccess;
     ok = ok && cudaStreamSynchronize(md->stream) == cudaSuccess;
@@ -680,6 +703,15 @@ int ds_model_destroy(ds_model* m) {
     delete m->md;
     delete m;
     return DS_OK;
+}
+
+int ds_model_set_wait_limit(ds_model* m, int polls) {
+    if (!m || polls < 0) return DS_ERR_ARG;
+    MlpModel* md = m->md;
+    if (cudaSetDevice(md->device) != cudaSuccess) return DS_ERR_CUDA;
+    const int v[2] = {0, polls};
+    if (cudaMemcpyAsync(md->err, v, sizeof(v), cudaMemcpyHostToDevice, md->stream) != cudaSuccess) return DS_ERR_CUDA;
+    return cudaStreamSynchronize(md->stream) == cudaSuccess ? DS_OK : DS_ERR_CUDA;
 }
 
 static int check_err(MlpModel* md) {

@@ -124,3 +124,34 @@ def test_singular_basis_reported(mode, case):
         assert abs(out[0] - 1.0) < 1e-15          # x_0 = rhs_0 / A[0, 0]
     finally:
         L_.ds_destroy(h)
+
+
+def test_scorer_wait_timeout_falls_back_to_dse():
+    """The scorer's bounded MMA-completion wait, made to run out by a one-poll
+    bound (ds_model_set_wait_limit): ds_solve returns DS_ERR_DEVICE_WAIT, the
+    timed-out iterations fall back to DSE pricing, and the solve still ends
+    optimal at the plain solve's objective.  With the default bound restored
+    the same handles solve cleanly."""
+    from parallel_ds_b200 import learned as LN
+    from parallel_ds_b200 import solver as S
+    from parallel_ds_b200._lib import DsError
+    L_ = lib()
+    lp = L.learned(2001)
+    plain = S.solve_lp(lp, pricing="dse")
+    model = LN.LeavingRowScorer.load()
+    assert L_.ds_model_set_wait_limit(model.h, 1) == 0
+    s = S.CudaDualSimplex(S.problem_from_lp(lp), pricing="learned", model=model)
+    s.initDualSimplex()
+    with pytest.raises(DsError) as ei:
+        s.solve()
+    assert ei.value.code == -6                         # DS_ERR_DEVICE_WAIT
+    assert s.status() == "optimal"
+    z = L_.ds_get_objective(s.h)
+    assert abs(z - plain["objective"]) <= 1e-9 * max(1.0, abs(plain["objective"]))
+    assert s.stats()["learned_fallback"] > 0
+    assert L_.ds_model_set_wait_limit(model.h, 0) == 0
+    s2 = S.CudaDualSimplex(S.problem_from_lp(lp), pricing="learned", model=model)
+    s2.initDualSimplex()
+    sol = s2.solve()
+    assert s2.status() == "optimal"
+    assert abs(sol.Z - plain["objective"]) <= 1e-9 * max(1.0, abs(plain["objective"]))
