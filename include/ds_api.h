@@ -339,6 +339,19 @@ int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, const double
 int ds_kernel_pfi_apply(int m, int T, const double* eta, const int* pos,
                         const double* rhs, double* sol, int transpose);
 
+/* Singleton triangularisation of a k x k sparse pattern (CSC col_ptr, row_idx;
+ * values not needed), the host stage of the eta-file mode's sparse LU of B0's
+ * structural block (it replaces the analysis phase of the reference's cuDSS
+ * factorisation, cudaSparseMatrix.cpp:502-567).  row_order and col_order (k
+ * each) receive the rows and columns in pivot order: the column singletons,
+ * then the kernel (rows and columns in index order), then the row singletons,
+ * so that the permuted matrix is block upper triangular around the kernel.
+ * *n_col1 and *n_kernel receive the counts of the first two groups.  Host
+ * only (no device work).  DS_ERR_NUMERIC if the pattern is structurally
+ * singular. */
+int ds_sparse_triangularise(int k, const int* col_ptr, const int* row_idx, int* row_order, int* col_order,
+                            int* n_col1, int* n_kernel);
+
 /* Device time in milliseconds (CUDA events on the default stream) of the
  * kernels that the calling thread's last ds_kernel_pivot_row or
  * ds_kernel_pfi_apply call launched, host copies excluded: the per-kernel

@@ -106,6 +106,7 @@ def lib():
                                            IP, IP, IP, DP, DP, IP]),
         "ds_kernel_pfi_apply": (C.c_int, [C.c_int, C.c_int, DP, IP, DP, DP, C.c_int]),
         "ds_kernel_last_time": (C.c_int, [DP]),
+        "ds_sparse_triangularise": (C.c_int, [C.c_int, IP, IP, IP, IP, IP, IP]),
         "ds_kernel_ratio_test_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                    IP, IP, DP, DP, IP, C.c_void_p]),

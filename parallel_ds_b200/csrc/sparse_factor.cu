@@ -443,6 +443,62 @@ std::vector<T> download(const T* p, size_t n, cudaStream_t s) {
 
 }  // namespace
 
+// Singleton triangularisation of a k x k pattern (CSC kc_*, CSR kr_* with the
+// entry index into the CSC in the CSR's order implied): column singletons of
+// the active part are pivoted first (in queue order), then row singletons;
+// the rows and columns left over form the kernel.  u1_e indexes the CSC entry
+// of a column-singleton pivot, u3_e the CSR entry of a row-singleton pivot.
+// Returns null, or why the pattern is structurally singular.
+const char* triangularise(int k, const int* kc_ptr, const int* kc_row, const int* kr_ptr, const int* kr_col,
+                          Triangular& T) {
+    std::vector<int> ccnt(k), rcnt(k), q;
+    T = Triangular{};
+    T.rdone.assign(k, 0);
+    T.cdone.assign(k, 0);
+    std::vector<char>& rdone = T.rdone;
+    std::vector<char>& cdone = T.cdone;
+    for (int j = 0; j < k; ++j) { ccnt[j] = kc_ptr[j + 1] - kc_ptr[j]; if (!ccnt[j]) return "empty column in the structural block"; }
+    for (int t = 0; t < k; ++t) { rcnt[t] = kr_ptr[t + 1] - kr_ptr[t]; if (!rcnt[t]) return "empty row in the structural block"; }
+    for (int j = 0; j < k; ++j) if (ccnt[j] == 1) q.push_back(j);
+    for (size_t h = 0; h < q.size(); ++h) {
+        const int j = q[h];
+        if (cdone[j] || ccnt[j] != 1) continue;
+        int t = -1, ex = -1;
+        for (int x = kc_ptr[j]; x < kc_ptr[j + 1]; ++x) if (!rdone[kc_row[x]]) { t = kc_row[x]; ex = x; break; }
+        if (t < 0) return "structurally singular structural block";
+        rdone[t] = 1; cdone[j] = 1;
+        T.u1_t.push_back(t); T.u1_j.push_back(j); T.u1_e.push_back(ex);
+        for (int y = kr_ptr[t]; y < kr_ptr[t + 1]; ++y) {
+            const int c = kr_col[y];
+            if (cdone[c]) continue;
+            if (--ccnt[c] == 1) q.push_back(c);
+            else if (ccnt[c] == 0) return "structurally singular structural block";
+        }
+    }
+    q.clear();
+    for (int t = 0; t < k; ++t) if (!rdone[t] && rcnt[t] == 1) q.push_back(t);
+    for (size_t h = 0; h < q.size(); ++h) {
+        const int t = q[h];
+        if (rdone[t] || rcnt[t] != 1) continue;
+        int j = -1, ey = -1;
+        for (int y = kr_ptr[t]; y < kr_ptr[t + 1]; ++y) if (!cdone[kr_col[y]]) { j = kr_col[y]; ey = y; break; }
+        if (j < 0) return "structurally singular structural block";
+        rdone[t] = 1; cdone[j] = 1;
+        T.u3_t.push_back(t); T.u3_j.push_back(j); T.u3_e.push_back(ey);
+        for (int x = kc_ptr[j]; x < kc_ptr[j + 1]; ++x) {
+            const int r = kc_row[x];
+            if (rdone[r]) continue;
+            if (--rcnt[r] == 1) q.push_back(r);
+            else if (rcnt[r] == 0) return "structurally singular structural block";
+        }
+    }
+    int kr = 0, kc = 0;
+    for (int t = 0; t < k; ++t) kr += !rdone[t];
+    for (int j = 0; j < k; ++j) kc += !cdone[j];
+    if (kr != kc) return "structurally singular structural block";
+    return nullptr;
+}
+
 SfInfo SparseLU::factor(const SfInput& in, const double* d_cval, cudaStream_t s, SfDev* out) {
     SfInfo info;
     const int k = in.k;
@@ -474,49 +530,16 @@ SfInfo SparseLU::factor(const SfInput& in, const double* d_cval, cudaStream_t s,
             for (int x = kc_ptr[j]; x < kc_ptr[j + 1]; ++x) { const int p = cur[kc_row[x]]++; kr_col[p] = j; kr_e[p] = kc_e[x]; }
     }
     // ---- triangularisation
-    std::vector<int> ccnt(k), rcnt(k);
-    std::vector<char> rdone(k, 0), cdone(k, 0);
-    for (int j = 0; j < k; ++j) { ccnt[j] = kc_ptr[j + 1] - kc_ptr[j]; if (!ccnt[j]) return fail("empty column in the structural block"); }
-    for (int t = 0; t < k; ++t) { rcnt[t] = kr_ptr[t + 1] - kr_ptr[t]; if (!rcnt[t]) return fail("empty row in the structural block"); }
-    std::vector<int> u1_t, u1_j, u1_e, u3_t, u3_j, u3_e, q;
-    for (int j = 0; j < k; ++j) if (ccnt[j] == 1) q.push_back(j);
-    for (size_t h = 0; h < q.size(); ++h) {
-        const int j = q[h];
-        if (cdone[j] || ccnt[j] != 1) continue;
-        int t = -1, ex = -1;
-        for (int x = kc_ptr[j]; x < kc_ptr[j + 1]; ++x) if (!rdone[kc_row[x]]) { t = kc_row[x]; ex = x; break; }
-        if (t < 0) return fail("structurally singular structural block");
-        rdone[t] = 1; cdone[j] = 1;
-        u1_t.push_back(t); u1_j.push_back(j); u1_e.push_back((int)ex);
-        for (int y = kr_ptr[t]; y < kr_ptr[t + 1]; ++y) {
-            const int c = kr_col[y];
-            if (cdone[c]) continue;
-            if (--ccnt[c] == 1) q.push_back(c);
-            else if (ccnt[c] == 0) return fail("structurally singular structural block");
-        }
-    }
-    q.clear();
-    for (int t = 0; t < k; ++t) if (!rdone[t] && rcnt[t] == 1) q.push_back(t);
-    for (size_t h = 0; h < q.size(); ++h) {
-        const int t = q[h];
-        if (rdone[t] || rcnt[t] != 1) continue;
-        int j = -1, ey = -1;
-        for (int y = kr_ptr[t]; y < kr_ptr[t + 1]; ++y) if (!cdone[kr_col[y]]) { j = kr_col[y]; ey = y; break; }
-        if (j < 0) return fail("structurally singular structural block");
-        rdone[t] = 1; cdone[j] = 1;
-        u3_t.push_back(t); u3_j.push_back(j); u3_e.push_back(ey);
-        for (int x = kc_ptr[j]; x < kc_ptr[j + 1]; ++x) {
-            const int r = kc_row[x];
-            if (rdone[r]) continue;
-            if (--rcnt[r] == 1) q.push_back(r);
-            else if (rcnt[r] == 0) return fail("structurally singular structural block");
-        }
-    }
+    Triangular tri;
+    if (const char* why = triangularise(k, kc_ptr.data(), kc_row.data(), kr_ptr.data(), kr_col.data(), tri))
+        return fail(why);
+    const std::vector<int>&u1_t = tri.u1_t, &u1_j = tri.u1_j, &u1_e = tri.u1_e;
+    const std::vector<int>&u3_t = tri.u3_t, &u3_j = tri.u3_j, &u3_e = tri.u3_e;
+    const std::vector<char>&rdone = tri.rdone, &cdone = tri.cdone;
     std::vector<int> krow, kcol, loc_row(k, -1), loc_col(k, -1);
     for (int t = 0; t < k; ++t) if (!rdone[t]) { loc_row[t] = (int)krow.size(); krow.push_back(t); }
     for (int j = 0; j < k; ++j) if (!cdone[j]) { loc_col[j] = (int)kcol.size(); kcol.push_back(j); }
     const int km = (int)krow.size();
-    if ((int)kcol.size() != km) return fail("structurally singular structural block");
     info.km = km;
     // ---- kernel LU on the device
     int ks = 0, kd = 0, nL = 0, pool_top = 0, Lcap = 1;
@@ -763,3 +786,38 @@ SfInfo SparseLU::factor(const SfInput& in, const double* d_cval, cudaStream_t s,
 }
 
 }  // namespace ds
+
+// Singleton triangularisation of a k x k sparse pattern (CSC col_ptr/row_idx),
+// for host-side tests: row_order and col_order list the rows and columns in
+// pivot order (column singletons, then the kernel's rows / columns in index
+// order, then the row singletons in reverse peel order), so that the permuted
+// matrix is block upper triangular around the kernel.  *n_col1 / *n_kernel
+// receive the counts.  DS_ERR_NUMERIC if the pattern is structurally singular.
+extern "C" int ds_sparse_triangularise(int k, const int* col_ptr, const int* row_idx, int* row_order, int* col_order,
+                                       int* n_col1, int* n_kernel) {
+    if (k <= 0 || !col_ptr || !row_idx || !row_order || !col_order || !n_col1 || !n_kernel) return DS_ERR_ARG;
+    const int nnz = col_ptr[k];
+    std::vector<int> rp(k + 1, 0), rc(nnz);
+    for (int x = 0; x < nnz; ++x) {
+        if (row_idx[x] < 0 || row_idx[x] >= k) return DS_ERR_ARG;
+        rp[row_idx[x] + 1]++;
+    }
+    for (int t = 0; t < k; ++t) rp[t + 1] += rp[t];
+    {
+        std::vector<int> cur(rp.begin(), rp.end() - 1);
+        for (int j = 0; j < k; ++j)
+            for (int x = col_ptr[j]; x < col_ptr[j + 1]; ++x) rc[cur[row_idx[x]]++] = j;
+    }
+    ds::Triangular T;
+    if (ds::triangularise(k, col_ptr, row_idx, rp.data(), rc.data(), T)) return DS_ERR_NUMERIC;
+    int w = 0;
+    for (size_t i = 0; i < T.u1_t.size(); ++i) { row_order[w] = T.u1_t[i]; col_order[w] = T.u1_j[i]; ++w; }
+    const int c1 = w;
+    int wr = w, wc = w;
+    for (int t = 0; t < k; ++t) if (!T.rdone[t]) row_order[wr++] = t;
+    for (int j = 0; j < k; ++j) if (!T.cdone[j]) col_order[wc++] = j;
+    for (int i = (int)T.u3_t.size() - 1; i >= 0; --i) { row_order[wr++] = T.u3_t[i]; col_order[wc++] = T.u3_j[i]; }
+    *n_col1 = c1;
+    *n_kernel = wr - c1 - (int)T.u3_t.size();
+    return DS_OK;
+}

@@ -37,6 +37,15 @@ struct SfInfo {
     char msg[160] = {0};
 };
 
+// Singleton triangularisation of the bump's pattern (sparse_factor.cu).
+struct Triangular {
+    std::vector<int> u1_t, u1_j, u1_e;   // column singletons: row, column, CSC entry (pivot order)
+    std::vector<int> u3_t, u3_j, u3_e;   // row singletons: row, column, CSR entry (peel order)
+    std::vector<char> rdone, cdone;      // rows / columns pivoted (the rest is the kernel)
+};
+const char* triangularise(int k, const int* kc_ptr, const int* kc_row, const int* kr_ptr, const int* kr_col,
+                          Triangular& T);
+
 class SparseLU {
 public:
     SparseLU() = default;
