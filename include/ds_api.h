@@ -117,7 +117,10 @@ typedef struct ds_stats {
     int    bump_size;          /* structurals in the last factorised basis         */
     int    kernel_launches;    /* kernels launched by the solve                    */
     double solve_ms;           /* device time of ds_solve (CUDA events)            */
-    double refactor_ms;        /* device time spent refactorising                  */
+    double refactor_ms;        /* time spent refactorising: device time of the dense
+                                  inverse; for the sparse LU the whole factorisation
+                                  (host triangularisation and program building, device
+                                  kernel LU), host wall time                       */
     double pdhg_ms;            /* device time of the PDHG warm-start estimate      */
     int    lu_kernel;          /* sparse LU, last factorisation: order of the bump's
                                   kernel left by the singleton triangularisation  */

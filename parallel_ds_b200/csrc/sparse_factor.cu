@@ -136,7 +136,8 @@ template <int BS>
 __global__ void __launch_bounds__(BS, 1) k_kernel_lu(KluArgs a) {
     __shared__ int sh_i[BS / 32 + 1];
     __shared__ long long sh_l[BS / 32];
-    __shared__ int s_npiv, s_err, s_round, s_top, s_nL;
+    __shared__ int s_npiv, s_err, s_round, s_nL;
+    __shared__ unsigned long long s_top;   // 64-bit: requests past an overflow must not wrap
     const int km = a.km;
     const int tid = threadIdx.x;
     for (int i = tid; i < km; i += BS) {
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(BS, 1) k_kernel_lu(KluArgs a) {
         }
         a.col_piv[i] = -1; a.row_piv[i] = -1;
     }
-    if (tid == 0) { s_npiv = 0; s_err = KLU_OK; s_round = 0; s_nL = 0; s_top = a.row_ptr[km] + 4 * km; }
+    if (tid == 0) { s_npiv = 0; s_err = KLU_OK; s_round = 0; s_nL = 0; s_top = (unsigned long long)(a.row_ptr[km] + 4 * km); }
     __syncthreads();
     while (a.sparse) {
         const int na = km - s_npiv;
@@ -280,8 +281,10 @@ __global__ void __launch_bounds__(BS, 1) k_kernel_lu(KluArgs a) {
                 const int nlen = len + fill;
                 if (nlen > a.r_cap[r]) {
                     const int ncap = max(2 * a.r_cap[r] + 4, nlen + 4);
-                    const int ns = atomicAdd(&s_top, ncap);
-                    if (ns > a.pool_cap - ncap) { atomicExch(&s_err, KLU_POOL_FULL); break; }
+                    if (*(volatile int*)&s_err != KLU_OK) break;   // the pool already overflowed
+                    const unsigned long long ns64 = atomicAdd(&s_top, (unsigned long long)ncap);
+                    if (ns64 + (unsigned long long)ncap > (unsigned long long)a.pool_cap) { atomicExch(&s_err, KLU_POOL_FULL); break; }
+                    const int ns = (int)ns64;
                     for (int x = 0; x < len; ++x) { a.pool_col[ns + x] = a.pool_col[st + x]; a.pool_val[ns + x] = a.pool_val[st + x]; }
                     st = ns;
                     a.r_start[r] = ns; a.r_cap[r] = ncap;
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(BS, 1) k_kernel_lu(KluArgs a) {
     if (tid == 0) {
         if (kd != kdc && s_err == KLU_OK) s_err = KLU_SINGULAR;
         a.out[0] = s_npiv; a.out[1] = min(s_nL, a.L_cap); a.out[2] = s_err; a.out[3] = s_round;
-        a.out[4] = s_top; a.out[5] = kd;
+        a.out[4] = (int)min(s_top, (unsigned long long)a.pool_cap); a.out[5] = kd;
     }
 }
 
