@@ -799,6 +799,9 @@ SfInfo SparseLU::factor(const SfInput& in, const double* d_cval, cudaStream_t s,
 extern "C" int ds_sparse_triangularise(int k, const int* col_ptr, const int* row_idx, int* row_order, int* col_order,
                                        int* n_col1, int* n_kernel) {
     if (k <= 0 || !col_ptr || !row_idx || !row_order || !col_order || !n_col1 || !n_kernel) return DS_ERR_ARG;
+    if (col_ptr[0] != 0) return DS_ERR_ARG;
+    for (int j = 0; j < k; ++j)
+        if (col_ptr[j + 1] < col_ptr[j]) return DS_ERR_ARG;
     const int nnz = col_ptr[k];
     std::vector<int> rp(k + 1, 0), rc(nnz);
     for (int x = 0; x < nnz; ++x) {

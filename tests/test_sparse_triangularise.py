@@ -91,3 +91,15 @@ def test_structurally_singular(case):
         A[1, 4] = 1.0
     rc, *_ = triangularise(A)
     assert rc == DS_ERR_NUMERIC
+
+
+def test_malformed_pattern_rejected():
+    k = 3
+    ro, co = np.zeros(k, np.int32), np.zeros(k, np.int32)
+    c1, km = C.c_int(), C.c_int()
+    for ptr_, idx in (([0, 2, 1, 3], [0, 1, 2]), ([1, 2, 3, 4], [0, 1, 2, 0]), ([0, 1, 2, 3], [0, 5, 2])):
+        p_ = np.asarray(ptr_, np.int32)
+        i_ = np.asarray(idx, np.int32)
+        rc = lib().ds_sparse_triangularise(k, ptr(p_, C.c_int), ptr(i_, C.c_int), ptr(ro, C.c_int),
+                                           ptr(co, C.c_int), C.byref(c1), C.byref(km))
+        assert rc == -1                            # DS_ERR_ARG
