@@ -67,6 +67,7 @@ struct Oracle {
 
     // factor of B0: K = A[rp_row, s_var], P K = L U
     int k = 0;
+    double min_pivot = 1e300, min_pivot_rel = 1e300, max_step = 0.0;   // phase-2 pivot statistics
     std::vector<int> s_pos, s_var, rp_row, row_slackpos, piv;
     std::vector<double> LU;
     // PFI eta file (PFIfactor / linalg::PFIsolve)
@@ -718,6 +719,13 @@ struct Oracle {
             }
             obj += dz;
             const double theta_P = delta / alpha_q[p_idx];
+            {
+                double amax = 0.0;
+                for (int i = 0; i < m; ++i) amax = std::max(amax, std::fabs(alpha_q[i]));
+                min_pivot = std::min(min_pivot, std::fabs(alpha_q[p_idx]));
+                if (amax > 0) min_pivot_rel = std::min(min_pivot_rel, std::fabs(alpha_q[p_idx]) / amax);
+                max_step = std::max(max_step, std::fabs(theta_P));
+            }
             // updateAndChangeBasis (sequentialDualSimplex.cpp:200-227)
             ftran(rho, tau);
             std::vector<double> ev(m);
@@ -803,6 +811,7 @@ int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const d
     double z = 0; for (int j = 0; j < n; ++j) z += (o.perturbed ? o.original_costs[j] : o.costs[j]) * o.x[j];
     res->objective = z;
     res->obj_incremental = o.obj;
+    res->min_pivot = o.min_pivot; res->min_pivot_rel = o.min_pivot_rel; res->max_step = o.max_step;
     if (x_out) std::memcpy(x_out, o.x.data(), sizeof(double) * o.N);
     if (d_out) std::memcpy(d_out, o.d.data(), sizeof(double) * o.N);
     if (basis_out) std::memcpy(basis_out, o.basis.data(), sizeof(int) * m);

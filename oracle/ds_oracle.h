@@ -39,6 +39,10 @@ typedef struct or_result {
     int bump_size;
     double objective;           /* c^T x over structurals (original costs)     */
     double obj_incremental;     /* reference obj_func_val after postProcess    */
+    /* pivot statistics of the phase-2 basis changes (numerical diagnostics) */
+    double min_pivot;           /* smallest |alpha_q[p]|                        */
+    double min_pivot_rel;       /* smallest |alpha_q[p]| / max_i |alpha_q[i]|   */
+    double max_step;            /* largest |theta_P| = |delta / alpha_q[p]|     */
 } or_result;
 
 void or_default_options(or_options* o);

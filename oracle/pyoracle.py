@@ -27,7 +27,8 @@ class OrResult(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("phase1_iterations", C.c_int),
                 ("refactors", C.c_int), ("restarts", C.c_int), ("perturbed", C.c_int),
                 ("bfrt_flips", C.c_int), ("bump_size", C.c_int),
-                ("objective", C.c_double), ("obj_incremental", C.c_double)]
+                ("objective", C.c_double), ("obj_incremental", C.c_double),
+                ("min_pivot", C.c_double), ("min_pivot_rel", C.c_double), ("max_step", C.c_double)]
 
 
 _lib = None
@@ -90,6 +91,7 @@ def solve_typed(lp, trace_cap=0, **opts):
                 phase1_iterations=r.phase1_iterations, refactors=r.refactors,
                 restarts=r.restarts, perturbed=bool(r.perturbed), bfrt_flips=r.bfrt_flips,
                 bump_size=r.bump_size, objective=r.objective, obj_incremental=r.obj_incremental,
+                min_pivot=r.min_pivot, min_pivot_rel=r.min_pivot_rel, max_step=r.max_step,
                 x=x, d=d, basis=basis, trace_count=cnt.value,
                 trace=dict(p=tp[:k].copy(), q=tq[:k].copy(), theta=tth[:k].copy(), obj=tob[:k].copy()))
 

@@ -141,3 +141,13 @@ def test_ratio_test_tie_rule():
     assert r["q_idx"] == 3 and r["num_candidates"] == 4
     d2 = d.copy(); d2[3] = 3.0 * (1 + 1e-11)      # now 3 ties with 2 but |alpha| 3 < 4
     assert po.ratio_test(nonbasis, alpha, 0.5, 0, x, d2, lb, ub, typ)["q_idx"] == 2
+
+
+def test_oracle_pivot_statistics():
+    """The oracle's numerical diagnostics: the smallest phase-2 pivot |alpha_q[p]|
+    (absolute and relative to its column) and the largest primal step."""
+    r = po.solve_typed(L.typed(L.plain_small(3)))
+    assert r["status"] == "optimal"
+    assert 0 < r["min_pivot_rel"] <= 1.0
+    assert r["min_pivot"] > 1e-5 * 0.999        # the ratio test only takes |alpha| > EPS_A
+    assert 0 < r["max_step"] < 1e12
