@@ -484,6 +484,19 @@ struct Oracle {
     // simpleRatioTest (tpp:546-572); q = -1 when nothing is taken (reference: uninitialised)
     void ratio_test(const std::vector<int>& F, const std::vector<double>& alpha, int& q, int& q_idx) const {
         q = -1; q_idx = -1;
+        if (opt.harris) {   // experiments: two-pass Harris (not the reference's rule)
+            double tmax = INF;
+            for (int i : F) {
+                const double a = alpha[i];
+                tmax = std::min(tmax, (d[nonbasis[i]] + std::copysign(EPS_D, a)) / a);
+            }
+            double best = -1.0;
+            for (int i : F) {
+                const int j = nonbasis[i];
+                if (d[j] / alpha[i] <= tmax && std::fabs(alpha[i]) > best) { best = std::fabs(alpha[i]); q = j; q_idx = i; }
+            }
+            return;
+        }
         double theta = INF;
         for (int i : F) {
             const int j = nonbasis[i];
@@ -690,7 +703,8 @@ struct Oracle {
             }
             if (q < 0) { status = ST_ERROR; throw Stop{}; }
             if (is_lower) for (double& a : alpha) a = -a;
-            const double theta = d[q] / alpha[q_idx];
+            double theta = d[q] / alpha[q_idx];
+            if (opt.harris && theta * sgn < 0) theta = 0.0;   // experiments: a wrong-signed step within the tolerance
             delta = sgn * delta;
             std::vector<double> aq(m, 0.0);
             for (int e2 = cptr[q]; e2 < cptr[q + 1]; ++e2) aq[crow[e2]] = cval[e2];
@@ -785,6 +799,7 @@ void or_default_options(or_options* o) {
     o->gpu_control_flow = 1;
     o->verbose = 0;
     o->var_weight = nullptr;
+    o->harris = 0;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,

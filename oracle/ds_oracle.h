@@ -26,6 +26,9 @@ typedef struct or_options {
     int verbose;
     const double* var_weight;   /* experiments: DSE score of row i is multiplied by
                                    var_weight[basis[i]] (NULL: plain DSE)          */
+    int harris;                 /* experiments: phase-2 ratio test by the two-pass
+                                   Harris rule (tolerance EPS_D) instead of the
+                                   reference's simpleRatioTest (0: reference)      */
 } or_options;
 
 typedef struct or_result {
