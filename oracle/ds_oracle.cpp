@@ -224,53 +224,310 @@ struct Oracle {
         if ((int)rp_row.size() != k) { status = ST_ERROR; throw Stop{}; }
         std::vector<int> rowk(m, -1);
         for (int t = 0; t < k; ++t) rowk[rp_row[t]] = t;
+        if (opt.block_lu) { block_factor(rowk); return; }
         LU.assign((size_t)k * k, 0.0);  // row-major K[t][j]
         for (int j = 0; j < k; ++j)
             for (int e = cptr[s_var[j]]; e < cptr[s_var[j] + 1]; ++e) {
                 int t = rowk[crow[e]];
                 if (t >= 0) LU[(size_t)t * k + j] = cval[e];
             }
-        piv.resize(k);
-        for (int c = 0; c < k; ++c) {
-            int pr = c; double best = std::fabs(LU[(size_t)c * k + c]);
-            for (int r = c + 1; r < k; ++r) { double v = std::fabs(LU[(size_t)r * k + c]); if (v > best) { best = v; pr = r; } }
-            piv[c] = pr;
-            if (!(best > 1e-14)) { status = ST_ERROR; throw Stop{}; }
-            if (pr != c) for (int j = 0; j < k; ++j) std::swap(LU[(size_t)c * k + j], LU[(size_t)pr * k + j]);
-            const double pv = LU[(size_t)c * k + c];
-            double* rowc = &LU[(size_t)c * k];
+        if (!dense_lu(LU, k, piv)) { status = ST_ERROR; throw Stop{}; }
+    }
+    // Dense LU with partial pivoting, row-major A (kk x kk), in place: PA = LU.
+    static bool dense_lu(std::vector<double>& A, int kk, std::vector<int>& pv) {
+        pv.resize(kk);
+        for (int c = 0; c < kk; ++c) {
+            int pr = c; double best = std::fabs(A[(size_t)c * kk + c]);
+            for (int r = c + 1; r < kk; ++r) { double v = std::fabs(A[(size_t)r * kk + c]); if (v > best) { best = v; pr = r; } }
+            pv[c] = pr;
+            if (!(best > 1e-14)) return false;
+            if (pr != c) for (int j = 0; j < kk; ++j) std::swap(A[(size_t)c * kk + j], A[(size_t)pr * kk + j]);
+            const double pvv = A[(size_t)c * kk + c];
+            double* rowc = &A[(size_t)c * kk];
 
-            for (int r = c + 1; r < k; ++r) {
-                double* rowr = &LU[(size_t)r * k];
-                const double l = rowr[c] / pv;
+            for (int r = c + 1; r < kk; ++r) {
+                double* rowr = &A[(size_t)r * kk];
+                const double l = rowr[c] / pvv;
                 rowr[c] = l;
                 if (l != 0.0)
-                    for (int j = c + 1; j < k; ++j) rowr[j] -= l * rowc[j];
+                    for (int j = c + 1; j < kk; ++j) rowr[j] -= l * rowc[j];
             }
         }
+        return true;
     }
-    // K z = b (b, z length k), PK = LU
-    void k_solve(std::vector<double>& z) const {
-        for (int c = 0; c < k; ++c) if (piv[c] != c) std::swap(z[c], z[piv[c]]);
-        for (int r = 0; r < k; ++r) { double s = z[r]; const double* row = &LU[(size_t)r * k]; for (int j = 0; j < r; ++j) s -= row[j] * z[j]; z[r] = s; }
-        for (int r = k - 1; r >= 0; --r) { double s = z[r]; const double* row = &LU[(size_t)r * k]; for (int j = r + 1; j < k; ++j) s -= row[j] * z[j]; z[r] = s / row[r]; }
+    // A z = b in place (PA = LU)
+    static void dense_solve(const std::vector<double>& A, int kk, const std::vector<int>& pv, double* z) {
+        for (int c = 0; c < kk; ++c) if (pv[c] != c) std::swap(z[c], z[pv[c]]);
+        for (int r = 0; r < kk; ++r) { double s = z[r]; const double* row = &A[(size_t)r * kk]; for (int j = 0; j < r; ++j) s -= row[j] * z[j]; z[r] = s; }
+        for (int r = kk - 1; r >= 0; --r) { double s = z[r]; const double* row = &A[(size_t)r * kk]; for (int j = r + 1; j < kk; ++j) s -= row[j] * z[j]; z[r] = s / row[r]; }
     }
-    // K^T z = b: U^T w = b, L^T v = w, z = P^T v
-    void kt_solve(std::vector<double>& z) const {
-        // row sweeps: U^T w = b, then L^T v = w (unit diagonal), then undo P
-        for (int j = 0; j < k; ++j) {
-            const double* row = &LU[(size_t)j * k];
+    // A^T z = b in place: U^T w = b, L^T v = w (unit diagonal), z = P^T v
+    static void dense_tsolve(const std::vector<double>& A, int kk, const std::vector<int>& pv, double* z) {
+        for (int j = 0; j < kk; ++j) {
+            const double* row = &A[(size_t)j * kk];
             const double wj = z[j] / row[j];
             z[j] = wj;
-            if (wj != 0.0) for (int r = j + 1; r < k; ++r) z[r] -= row[r] * wj;
+            if (wj != 0.0) for (int r = j + 1; r < kk; ++r) z[r] -= row[r] * wj;
         }
-        for (int j = k - 1; j >= 0; --j) {
-            const double* row = &LU[(size_t)j * k];
+        for (int j = kk - 1; j >= 0; --j) {
+            const double* row = &A[(size_t)j * kk];
             const double vj = z[j];
             if (vj != 0.0) for (int r = 0; r < j; ++r) z[r] -= row[r] * vj;
         }
-        for (int c = k - 1; c >= 0; --c) if (piv[c] != c) std::swap(z[c], z[piv[c]]);
+        for (int c = kk - 1; c >= 0; --c) if (pv[c] != c) std::swap(z[c], z[pv[c]]);
     }
+    // K z = b (b, z length k), PK = LU
+    void k_solve(std::vector<double>& z) const {
+        if (opt.block_lu) { block_solve(z); return; }
+        dense_solve(LU, k, piv, z.data());
+    }
+    // K^T z = b
+    void kt_solve(std::vector<double>& z) const {
+        if (opt.block_lu) { block_tsolve(z); return; }
+        dense_tsolve(LU, k, piv, z.data());
+    }
+    // ---- experiments (opt.block_lu): K put in block upper triangular form by its
+    // column singletons (first) and row singletons (last), the kernel left in
+    // between factorised by the dense LU above; values straight from A.
+    std::vector<int> bk_cptr, bk_crow, bk_rptr, bk_rcol, bt_u1t, bt_u1j, bt_u3t, bt_u3j, bt_krow, bt_kcol, bt_piv;
+    std::vector<double> bk_cval, bk_rval, bt_M;
+    std::vector<char> bt_u3col, bt_u1row;
+    int bt_km = 0;
+    // block_lu == 2: the kernel by sequential Markowitz with threshold pivoting
+    std::vector<int> sk_prow, sk_pcol, sk_uptr, sk_ucol, sk_lptr, sk_lrow;
+    std::vector<double> sk_uval, sk_lval, sk_udiag;
+    std::vector<std::vector<std::pair<int, double>>> sk_rows;
+    bool sparse_kernel_lu() {
+        const int km = bt_km;
+        std::vector<std::vector<std::pair<int, double>>>& rows = sk_rows;
+        std::vector<std::vector<int>> cols(km);
+        for (int a = 0; a < km; ++a)
+            for (const auto& e : rows[a]) cols[e.first].push_back(a);
+        std::vector<char> rdone(km, 0), cdone(km, 0);
+        sk_prow.clear(); sk_pcol.clear(); sk_uptr.assign(1, 0); sk_ucol.clear(); sk_uval.clear(); sk_udiag.clear();
+        sk_lptr.assign(1, 0); sk_lrow.clear(); sk_lval.clear();
+        auto value = [&](int r, int c) {
+            for (const auto& e : rows[r]) if (e.first == c) return e.second;
+            return 0.0;
+        };
+        for (int step = 0; step < km; ++step) {
+            // the columns of fewest active entries (up to four), their admissible rows of least cost
+            int cmin = INT32_MAX;
+            std::vector<int> cnt(km, 0);
+            for (int b = 0; b < km; ++b) {
+                if (cdone[b]) continue;
+                int c2 = 0;
+                for (int r : cols[b]) if (!rdone[r] && value(r, b) != 0.0) ++c2;
+                cnt[b] = c2;
+                if (c2 < cmin) cmin = c2;
+            }
+            if (cmin == 0 || cmin == INT32_MAX) return false;
+            long best = -1; int bi = -1, bj = -1, seen = 0;
+            for (int b = 0; b < km && seen < 4; ++b) {
+                if (cdone[b] || cnt[b] != cmin) continue;
+                ++seen;
+                double mx = 0.0;
+                for (int r : cols[b]) if (!rdone[r]) mx = std::max(mx, std::fabs(value(r, b)));
+                for (int r : cols[b]) {
+                    if (rdone[r]) continue;
+                    const double v = value(r, b);
+                    if (v == 0.0 || std::fabs(v) < 0.1 * mx) continue;
+                    const long cost = (long)((int)rows[r].size() - 1) * (cmin - 1);
+                    if (best < 0 || cost < best || (cost == best && (r < bi || (r == bi && b < bj)))) { best = cost; bi = r; bj = b; }
+                }
+            }
+            if (bi < 0) return false;
+            const double pv = value(bi, bj);
+            if (!(std::fabs(pv) > 1e-14)) return false;
+            sk_prow.push_back(bi); sk_pcol.push_back(bj); sk_udiag.push_back(pv);
+            for (const auto& e : rows[bi]) if (e.first != bj) { sk_ucol.push_back(e.first); sk_uval.push_back(e.second); }
+            sk_uptr.push_back((int)sk_ucol.size());
+            rdone[bi] = 1; cdone[bj] = 1;
+            for (int r : cols[bj]) {
+                if (rdone[r]) continue;
+                const double arj = value(r, bj);
+                if (arj == 0.0) continue;
+                const double l = arj / pv;
+                sk_lrow.push_back(r); sk_lval.push_back(l);
+                // row r <- row r - l * row bi (the pivot column's entry dropped)
+                std::vector<std::pair<int, double>> nr;
+                size_t x = 0, y = 0;
+                const auto& R = rows[r];
+                const auto& P = rows[bi];
+                while (x < R.size() || y < P.size()) {
+                    if (y == P.size() || (x < R.size() && R[x].first < P[y].first)) { if (R[x].first != bj) nr.push_back(R[x]); ++x; }
+                    else if (x == R.size() || P[y].first < R[x].first) {
+                        if (P[y].first != bj) { nr.push_back({P[y].first, -l * P[y].second}); cols[P[y].first].push_back(r); }
+                        ++y;
+                    } else {
+                        if (R[x].first != bj) nr.push_back({R[x].first, R[x].second - l * P[y].second});
+                        ++x; ++y;
+                    }
+                }
+                rows[r].swap(nr);
+            }
+            sk_lptr.push_back((int)sk_lrow.size());
+        }
+        return true;
+    }
+    // kernel M w = b (b by kernel row in, w by kernel column out)
+    void sparse_kernel_solve(double* z) const {
+        const int km = bt_km;
+        std::vector<double> b(z, z + km), x(km, 0.0);
+        for (int st = 0; st < km; ++st) {
+            const double bp = b[sk_prow[st]];
+            for (int e = sk_lptr[st]; e < sk_lptr[st + 1]; ++e) b[sk_lrow[e]] -= sk_lval[e] * bp;
+        }
+        for (int st = km - 1; st >= 0; --st) {
+            double v = b[sk_prow[st]];
+            for (int e = sk_uptr[st]; e < sk_uptr[st + 1]; ++e) v -= sk_uval[e] * x[sk_ucol[e]];
+            x[sk_pcol[st]] = v / sk_udiag[st];
+        }
+        for (int i = 0; i < km; ++i) z[i] = x[i];
+    }
+    // kernel M^T y = c (c by kernel column in, y by kernel row out)
+    void sparse_kernel_tsolve(double* z) const {
+        const int km = bt_km;
+        std::vector<double> c(z, z + km), w(km, 0.0), y(km, 0.0);
+        for (int st = 0; st < km; ++st) {
+            const double ws = c[sk_pcol[st]] / sk_udiag[st];
+            w[st] = ws;
+            for (int e = sk_uptr[st]; e < sk_uptr[st + 1]; ++e) c[sk_ucol[e]] -= sk_uval[e] * ws;
+        }
+        for (int st = km - 1; st >= 0; --st) {
+            double v = w[st];
+            for (int e = sk_lptr[st]; e < sk_lptr[st + 1]; ++e) v -= sk_lval[e] * y[sk_lrow[e]];
+            y[sk_prow[st]] = v;
+        }
+        for (int i = 0; i < km; ++i) z[i] = y[i];
+    }
+    void block_factor(const std::vector<int>& rowk) {
+        bk_cptr.assign(k + 1, 0); bk_crow.clear(); bk_cval.clear();
+        for (int j = 0; j < k; ++j) {
+            for (int e = cptr[s_var[j]]; e < cptr[s_var[j] + 1]; ++e) {
+                const int t = rowk[crow[e]];
+                if (t >= 0 && cval[e] != 0.0) { bk_crow.push_back(t); bk_cval.push_back(cval[e]); }
+            }
+            bk_cptr[j + 1] = (int)bk_crow.size();
+        }
+        const int nz = bk_cptr[k];
+        bk_rptr.assign(k + 1, 0); bk_rcol.assign(nz, 0); bk_rval.assign(nz, 0.0);
+        for (int x = 0; x < nz; ++x) bk_rptr[bk_crow[x] + 1]++;
+        for (int t = 0; t < k; ++t) bk_rptr[t + 1] += bk_rptr[t];
+        {
+            std::vector<int> cur(bk_rptr.begin(), bk_rptr.end() - 1);
+            for (int j = 0; j < k; ++j)
+                for (int x = bk_cptr[j]; x < bk_cptr[j + 1]; ++x) { const int q = cur[bk_crow[x]]++; bk_rcol[q] = j; bk_rval[q] = bk_cval[x]; }
+        }
+        std::vector<int> ccnt(k), rcnt(k), qu;
+        std::vector<char> rdone(k, 0), cdone(k, 0);
+        bt_u1t.clear(); bt_u1j.clear(); bt_u3t.clear(); bt_u3j.clear();
+        auto singular = [&]() { status = ST_ERROR; throw Stop{}; };
+        for (int j = 0; j < k; ++j) { ccnt[j] = bk_cptr[j + 1] - bk_cptr[j]; if (!ccnt[j]) singular(); if (ccnt[j] == 1) qu.push_back(j); }
+        for (int t = 0; t < k; ++t) { rcnt[t] = bk_rptr[t + 1] - bk_rptr[t]; if (!rcnt[t]) singular(); }
+        for (size_t h = 0; h < qu.size(); ++h) {
+            const int j = qu[h];
+            if (cdone[j] || ccnt[j] != 1) continue;
+            int t = -1;
+            for (int x = bk_cptr[j]; x < bk_cptr[j + 1]; ++x) if (!rdone[bk_crow[x]]) { t = bk_crow[x]; break; }
+            if (t < 0) singular();
+            rdone[t] = 1; cdone[j] = 1; bt_u1t.push_back(t); bt_u1j.push_back(j);
+            for (int y = bk_rptr[t]; y < bk_rptr[t + 1]; ++y) {
+                const int c = bk_rcol[y];
+                if (cdone[c]) continue;
+                if (--ccnt[c] == 1) qu.push_back(c); else if (ccnt[c] == 0) singular();
+            }
+        }
+        qu.clear();
+        for (int t = 0; t < k; ++t) if (!rdone[t] && rcnt[t] == 1) qu.push_back(t);
+        for (size_t h = 0; h < qu.size(); ++h) {
+            const int t = qu[h];
+            if (rdone[t] || rcnt[t] != 1) continue;
+            int j = -1;
+            for (int y = bk_rptr[t]; y < bk_rptr[t + 1]; ++y) if (!cdone[bk_rcol[y]]) { j = bk_rcol[y]; break; }
+            if (j < 0) singular();
+            rdone[t] = 1; cdone[j] = 1; bt_u3t.push_back(t); bt_u3j.push_back(j);
+            for (int x = bk_cptr[j]; x < bk_cptr[j + 1]; ++x) {
+                const int r = bk_crow[x];
+                if (rdone[r]) continue;
+                if (--rcnt[r] == 1) qu.push_back(r); else if (rcnt[r] == 0) singular();
+            }
+        }
+        bt_krow.clear(); bt_kcol.clear();
+        std::vector<int> kcl(k, -1);
+        for (int t = 0; t < k; ++t) if (!rdone[t]) bt_krow.push_back(t);
+        for (int j = 0; j < k; ++j) if (!cdone[j]) { kcl[j] = (int)bt_kcol.size(); bt_kcol.push_back(j); }
+        bt_km = (int)bt_krow.size();
+        if ((int)bt_kcol.size() != bt_km) singular();
+        bt_u3col.assign(k, 0); bt_u1row.assign(k, 0);
+        for (int j : bt_u3j) bt_u3col[j] = 1;
+        for (int t : bt_u1t) bt_u1row[t] = 1;
+        if (opt.block_lu == 2) {   // kernel rows kept sparse, sorted by kernel column
+            sk_rows.assign(bt_km, {});
+            for (int a = 0; a < bt_km; ++a)
+                for (int y = bk_rptr[bt_krow[a]]; y < bk_rptr[bt_krow[a] + 1]; ++y)
+                    if (kcl[bk_rcol[y]] >= 0) sk_rows[a].push_back({kcl[bk_rcol[y]], bk_rval[y]});
+        } else {
+            bt_M.assign((size_t)bt_km * bt_km, 0.0);
+            for (int a = 0; a < bt_km; ++a)
+                for (int y = bk_rptr[bt_krow[a]]; y < bk_rptr[bt_krow[a] + 1]; ++y)
+                    if (kcl[bk_rcol[y]] >= 0) bt_M[(size_t)a * bt_km + kcl[bk_rcol[y]]] = bk_rval[y];
+        }
+        if (bt_km > 0 && !(opt.block_lu == 2 ? sparse_kernel_lu() : dense_lu(bt_M, bt_km, bt_piv))) singular();
+    }
+    // K x = b: b by K rows in, x by K columns out
+    void block_solve(std::vector<double>& z) const {
+        const std::vector<double> b = z;
+        std::vector<double> x(k, 0.0);
+        auto row_step = [&](int t, int j) {
+            double s = b[t], pv = 0.0;
+            for (int y = bk_rptr[t]; y < bk_rptr[t + 1]; ++y) {
+                if (bk_rcol[y] == j) pv = bk_rval[y]; else s -= bk_rval[y] * x[bk_rcol[y]];
+            }
+            x[j] = s / pv;
+        };
+        for (size_t i = 0; i < bt_u3t.size(); ++i) row_step(bt_u3t[i], bt_u3j[i]);
+        if (bt_km > 0) {
+            std::vector<double> w(bt_km);
+            for (int a = 0; a < bt_km; ++a) {
+                const int t = bt_krow[a];
+                double s = b[t];
+                for (int y = bk_rptr[t]; y < bk_rptr[t + 1]; ++y) if (bt_u3col[bk_rcol[y]]) s -= bk_rval[y] * x[bk_rcol[y]];
+                w[a] = s;
+            }
+            if (opt.block_lu == 2) sparse_kernel_solve(w.data()); else dense_solve(bt_M, bt_km, bt_piv, w.data());
+            for (int c = 0; c < bt_km; ++c) x[bt_kcol[c]] = w[c];
+        }
+        for (int i = (int)bt_u1t.size() - 1; i >= 0; --i) row_step(bt_u1t[i], bt_u1j[i]);
+        z = x;
+    }
+    // K^T y = c: c by K columns in, y by K rows out
+    void block_tsolve(std::vector<double>& z) const {
+        const std::vector<double> c = z;
+        std::vector<double> y(k, 0.0);
+        auto col_step = [&](int t, int j) {
+            double s = c[j], pv = 0.0;
+            for (int x = bk_cptr[j]; x < bk_cptr[j + 1]; ++x) {
+                if (bk_crow[x] == t) pv = bk_cval[x]; else s -= bk_cval[x] * y[bk_crow[x]];
+            }
+            y[t] = s / pv;
+        };
+        for (size_t i = 0; i < bt_u1t.size(); ++i) col_step(bt_u1t[i], bt_u1j[i]);
+        if (bt_km > 0) {
+            std::vector<double> g(bt_km);
+            for (int b2 = 0; b2 < bt_km; ++b2) {
+                const int j = bt_kcol[b2];
+                double s = c[j];
+                for (int x = bk_cptr[j]; x < bk_cptr[j + 1]; ++x) if (bt_u1row[bk_crow[x]]) s -= bk_cval[x] * y[bk_crow[x]];
+                g[b2] = s;
+            }
+            if (opt.block_lu == 2) sparse_kernel_tsolve(g.data()); else dense_tsolve(bt_M, bt_km, bt_piv, g.data());
+            for (int a = 0; a < bt_km; ++a) y[bt_krow[a]] = g[a];
+        }
+        for (int i = (int)bt_u3t.size() - 1; i >= 0; --i) col_step(bt_u3t[i], bt_u3j[i]);
+        z = y;
+    }
+
     // B0 x = b (b by rows, x by positions): Matrix::solve non-transposed.
     void b0_solve(const std::vector<double>& b, std::vector<double>& out) const {
         std::vector<double> z(k);
@@ -800,6 +1057,7 @@ void or_default_options(or_options* o) {
     o->verbose = 0;
     o->var_weight = nullptr;
     o->harris = 0;
+    o->block_lu = 0;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,

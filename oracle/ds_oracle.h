@@ -29,6 +29,10 @@ typedef struct or_options {
     int harris;                 /* experiments: phase-2 ratio test by the two-pass
                                    Harris rule (tolerance EPS_D) instead of the
                                    reference's simpleRatioTest (0: reference)      */
+    int block_lu;               /* experiments: factorise the structural block by
+                                   singleton triangularisation + an LU of the
+                                   kernel only: 1 dense, 2 sequential Markowitz
+                                   (0: dense LU of the whole block)             */
 } or_options;
 
 typedef struct or_result {
