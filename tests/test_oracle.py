@@ -151,3 +151,16 @@ def test_oracle_pivot_statistics():
     assert 0 < r["min_pivot_rel"] <= 1.0
     assert r["min_pivot"] > 1e-5 * 0.999        # the ratio test only takes |alpha| > EPS_A
     assert 0 < r["max_step"] < 1e12
+
+
+@pytest.mark.parametrize("block_lu", [1, 2])
+def test_oracle_block_factorisation(block_lu):
+    """The oracle's experimental factorisations of the structural block
+    (singleton triangularisation + dense or Markowitz kernel LU) reach HiGHS's
+    optimum like its default dense LU."""
+    from parallel_ds_b200 import _lib
+    for lp in (L.plain_small(1), L.generate(_lib.GEN_PER_COL, 600, 1200, per_col=8, seed=2)):
+        h = highs(lp)
+        r = po.solve_typed(L.typed(lp), block_lu=block_lu)
+        assert r["status"] == "optimal"
+        assert abs(r["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
