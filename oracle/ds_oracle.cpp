@@ -941,6 +941,13 @@ struct Oracle {
                 else cond = type[j] == FREE;
                 if (cond) F.push_back(i);
             }
+            if (opt.rt_rel_tol > 0 && !F.empty()) {   // experiments: drop relatively tiny pivots
+                double amax = 0.0;
+                for (int i : F) amax = std::max(amax, std::fabs(alpha[i]));
+                std::vector<int> F2;
+                for (int i : F) if (std::fabs(alpha[i]) >= opt.rt_rel_tol * amax) F2.push_back(i);
+                F.swap(F2);
+            }
             if (F.empty()) {
                 if (unbound_checked) { status = ST_PRIMAL_INF; break; }
                 unbound_checked = true;
@@ -1058,6 +1065,7 @@ void or_default_options(or_options* o) {
     o->var_weight = nullptr;
     o->harris = 0;
     o->block_lu = 0;
+    o->rt_rel_tol = 0.0;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,

@@ -33,6 +33,9 @@ typedef struct or_options {
                                    singleton triangularisation + an LU of the
                                    kernel only: 1 dense, 2 sequential Markowitz
                                    (0: dense LU of the whole block)             */
+    double rt_rel_tol;          /* experiments: phase-2 ratio-test candidates with
+                                   |alpha_j| below this fraction of the largest
+                                   candidate |alpha| are left out (0: reference) */
 } or_options;
 
 typedef struct or_result {

@@ -21,7 +21,7 @@ class OrOptions(C.Structure):
     _fields_ = [("refactor_interval", C.c_int), ("max_iterations", C.c_int),
                 ("strict_reference", C.c_int), ("seed", C.c_ulonglong),
                 ("gpu_control_flow", C.c_int), ("verbose", C.c_int), ("var_weight", C.c_void_p),
-                ("harris", C.c_int), ("block_lu", C.c_int)]
+                ("harris", C.c_int), ("block_lu", C.c_int), ("rt_rel_tol", C.c_double)]
 
 
 class OrResult(C.Structure):
