@@ -68,6 +68,8 @@ struct Oracle {
     // factor of B0: K = A[rp_row, s_var], P K = L U
     int k = 0;
     double min_pivot = 1e300, min_pivot_rel = 1e300, max_step = 0.0;   // phase-2 pivot statistics
+    std::vector<int> p2_block;   // experiments (col_rel_tol): iteration until which a position is not priced
+    int refused_pivots = 0;
     std::vector<int> s_pos, s_var, rp_row, row_slackpos, piv;
     std::vector<double> LU;
     // PFI eta file (PFIfactor / linalg::PFIsolve)
@@ -908,12 +910,18 @@ struct Oracle {
             // DSEPricing (tpp:470-501); blocked set is always empty in phase 2
             double maxw = 0, delta = 0; int p = -1, p_idx = -1; bool is_lower = false;
             for (int i = 0; i < m; ++i) {
+                if (!p2_block.empty() && p2_block[i] > iteration) continue;   // experiments (col_rel_tol)
                 auto [inf, dt] = var_infeas(basis[i]);
                 if (inf && std::fabs(dt) > 1e-8) {
                     double w = (dt * dt) / beta[i];
                     if (opt.var_weight) w *= opt.var_weight[basis[i]];
                     if (w > maxw) { p = basis[i]; p_idx = i; delta = dt; maxw = w; is_lower = dt < 0; }
                 }
+            }
+            if ((p < 0 || p_idx < 0) && !p2_block.empty()) {   // experiments: blocked rows come back first
+                bool any = false;
+                for (int& b : p2_block) { any |= b > iteration; b = 0; }
+                if (any) continue;
             }
             if (p < 0 || p_idx < 0) {
                 if (!opt.strict_reference && pivots_at_nop == pivots) {
@@ -973,6 +981,17 @@ struct Oracle {
             std::vector<double> aq(m, 0.0);
             for (int e2 = cptr[q]; e2 < cptr[q + 1]; ++e2) aq[crow[e2]] = cval[e2];
             ftran(aq, alpha_q);
+            if (opt.col_rel_tol > 0) {   // experiments: refuse a pivot tiny against its column
+                double amax = 0.0;
+                for (double v : alpha_q) amax = std::max(amax, std::fabs(v));
+                if (std::fabs(alpha_q[p_idx]) < opt.col_rel_tol * amax) {
+                    if (p2_block.empty()) p2_block.assign(m, 0);
+                    p2_block[p_idx] = iteration + 100;
+                    ++refused_pivots;
+                    refactor();
+                    continue;
+                }
+            }
             if (std::fabs(alpha_q[p_idx] - alpha[q_idx]) > EPS_R * (1 + std::fabs(alpha_q[p_idx]))) refactor();
             // dual update + BFRT sets (sequentialDualSimplex.cpp:438-467)
             std::vector<int> low, up;
@@ -1066,6 +1085,7 @@ void or_default_options(or_options* o) {
     o->harris = 0;
     o->block_lu = 0;
     o->rt_rel_tol = 0.0;
+    o->col_rel_tol = 0.0;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,
@@ -1093,6 +1113,7 @@ int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const d
     res->objective = z;
     res->obj_incremental = o.obj;
     res->min_pivot = o.min_pivot; res->min_pivot_rel = o.min_pivot_rel; res->max_step = o.max_step;
+    res->refused_pivots = o.refused_pivots;
     if (x_out) std::memcpy(x_out, o.x.data(), sizeof(double) * o.N);
     if (d_out) std::memcpy(d_out, o.d.data(), sizeof(double) * o.N);
     if (basis_out) std::memcpy(basis_out, o.basis.data(), sizeof(int) * m);

@@ -36,6 +36,10 @@ typedef struct or_options {
     double rt_rel_tol;          /* experiments: phase-2 ratio-test candidates with
                                    |alpha_j| below this fraction of the largest
                                    candidate |alpha| are left out (0: reference) */
+    double col_rel_tol;         /* experiments: a phase-2 pivot |alpha_q[p]| below
+                                   this fraction of max_i |alpha_q[i]| is refused:
+                                   the factor is rebuilt and row p is left out of
+                                   pricing for 100 iterations (0: reference)    */
 } or_options;
 
 typedef struct or_result {
@@ -53,6 +57,7 @@ typedef struct or_result {
     double min_pivot;           /* smallest |alpha_q[p]|                        */
     double min_pivot_rel;       /* smallest |alpha_q[p]| / max_i |alpha_q[i]|   */
     double max_step;            /* largest |theta_P| = |delta / alpha_q[p]|     */
+    int refused_pivots;         /* experiments (col_rel_tol): pivots refused    */
 } or_result;
 
 void or_default_options(or_options* o);

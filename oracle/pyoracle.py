@@ -21,7 +21,8 @@ class OrOptions(C.Structure):
     _fields_ = [("refactor_interval", C.c_int), ("max_iterations", C.c_int),
                 ("strict_reference", C.c_int), ("seed", C.c_ulonglong),
                 ("gpu_control_flow", C.c_int), ("verbose", C.c_int), ("var_weight", C.c_void_p),
-                ("harris", C.c_int), ("block_lu", C.c_int), ("rt_rel_tol", C.c_double)]
+                ("harris", C.c_int), ("block_lu", C.c_int), ("rt_rel_tol", C.c_double),
+                ("col_rel_tol", C.c_double)]
 
 
 class OrResult(C.Structure):
@@ -29,7 +30,8 @@ class OrResult(C.Structure):
                 ("refactors", C.c_int), ("restarts", C.c_int), ("perturbed", C.c_int),
                 ("bfrt_flips", C.c_int), ("bump_size", C.c_int),
                 ("objective", C.c_double), ("obj_incremental", C.c_double),
-                ("min_pivot", C.c_double), ("min_pivot_rel", C.c_double), ("max_step", C.c_double)]
+                ("min_pivot", C.c_double), ("min_pivot_rel", C.c_double), ("max_step", C.c_double),
+                ("refused_pivots", C.c_int)]
 
 
 _lib = None
@@ -93,6 +95,7 @@ def solve_typed(lp, trace_cap=0, **opts):
                 restarts=r.restarts, perturbed=bool(r.perturbed), bfrt_flips=r.bfrt_flips,
                 bump_size=r.bump_size, objective=r.objective, obj_incremental=r.obj_incremental,
                 min_pivot=r.min_pivot, min_pivot_rel=r.min_pivot_rel, max_step=r.max_step,
+                refused_pivots=r.refused_pivots,
                 x=x, d=d, basis=basis, trace_count=cnt.value,
                 trace=dict(p=tp[:k].copy(), q=tq[:k].copy(), theta=tth[:k].copy(), obj=tob[:k].copy()))
 
