@@ -940,12 +940,13 @@ struct Oracle {
             const int sgn = is_lower ? -1 : 1;
             if (is_lower) for (double& a : alpha) a = -a;
             std::vector<int> F; F.reserve(n);
+            const double eps_a = opt.pivot_abs_tol > 0 ? opt.pivot_abs_tol : EPS_A;   // experiments
             for (int i = 0; i < n; ++i) {
                 bool cond = false;
                 const double a = alpha[i];
                 const int j = nonbasis[i];
-                if (a > EPS_A) cond = std::fabs(x[j] - lb[j]) < EPS_Z && (type[j] == LOWER || type[j] == BOXED);
-                else if (a < -EPS_A) cond = std::fabs(x[j] - ub[j]) < EPS_Z && (type[j] == UPPER || type[j] == BOXED);
+                if (a > eps_a) cond = std::fabs(x[j] - lb[j]) < EPS_Z && (type[j] == LOWER || type[j] == BOXED);
+                else if (a < -eps_a) cond = std::fabs(x[j] - ub[j]) < EPS_Z && (type[j] == UPPER || type[j] == BOXED);
                 else cond = type[j] == FREE;
                 if (cond) F.push_back(i);
             }
@@ -1086,6 +1087,7 @@ void or_default_options(or_options* o) {
     o->block_lu = 0;
     o->rt_rel_tol = 0.0;
     o->col_rel_tol = 0.0;
+    o->pivot_abs_tol = 0.0;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,

@@ -40,6 +40,9 @@ typedef struct or_options {
                                    this fraction of max_i |alpha_q[i]| is refused:
                                    the factor is rebuilt and row p is left out of
                                    pricing for 100 iterations (0: reference)    */
+    double pivot_abs_tol;       /* experiments: phase-2 ratio-test candidates need
+                                   |alpha_j| above this instead of EPS_A = 1e-5
+                                   (0: reference)                              */
 } or_options;
 
 typedef struct or_result {
