@@ -643,6 +643,18 @@ struct Oracle {
         return num;
     }
     bool dual_feasible() const { return dual_infeasible_count() == 0; }
+    // experiments (shift_costs): make every wrong-signed nonbasic reduced cost a
+    // small margin of the right sign by shifting its cost; false if a free
+    // variable is dual infeasible (no shift fixes that)
+    bool shift_dual_infeasible() {
+        for (int j : nonbasis) {
+            const double margin = 1e-7 + 1e-5 * std::fabs(original_costs.empty() ? costs[j] : original_costs[j]);
+            if (type[j] == LOWER && d[j] < -EPS_D) { costs[j] += -d[j] + margin; d[j] = margin; }
+            else if (type[j] == UPPER && d[j] > EPS_D) { costs[j] += -d[j] - margin; d[j] = -margin; }
+            else if (type[j] == FREE && std::fabs(d[j]) < EPS_D) return false;
+        }
+        return dual_feasible();
+    }
 
     // setPrimalVars (tpp:74-101)
     void set_primal_vars() {
@@ -899,12 +911,16 @@ struct Oracle {
             ++iteration; tick();
             if (iteration % opt.refactor_interval == 0) refactor();
             if (iteration % NEED_RESTART == 0 && !dual_feasible()) {
-                refactor(); phase1(); dual_simplex_init(); ++restarts;
+                if (!(opt.shift_costs && perturbed && shift_dual_infeasible())) {
+                    refactor(); phase1(); dual_simplex_init(); ++restarts;
+                }
             }
             if (!perturbed && cycle > MAX_CYCLE) {
                 perturb(); refactor(); dual_simplex_init();
                 // guard: the perturbed reduced costs may be dual infeasible
-                if (!opt.strict_reference && !dual_feasible()) { refactor(); phase1(); dual_simplex_init(); ++restarts; }
+                if (!opt.strict_reference && !dual_feasible() && !(opt.shift_costs && shift_dual_infeasible())) {
+                    refactor(); phase1(); dual_simplex_init(); ++restarts;
+                }
             }
             if (primal_feasible()) { status = ST_OPTIMAL; break; }
             // DSEPricing (tpp:470-501); blocked set is always empty in phase 2
@@ -1088,6 +1104,7 @@ void or_default_options(or_options* o) {
     o->rt_rel_tol = 0.0;
     o->col_rel_tol = 0.0;
     o->pivot_abs_tol = 0.0;
+    o->shift_costs = 0;
 }
 
 int or_solve_typed(int m, int n, const int* row_ptr, const int* col_idx, const double* val,

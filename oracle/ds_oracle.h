@@ -43,6 +43,9 @@ typedef struct or_options {
     double pivot_abs_tol;       /* experiments: phase-2 ratio-test candidates need
                                    |alpha_j| above this instead of EPS_A = 1e-5
                                    (0: reference)                              */
+    int shift_costs;            /* experiments: once the costs are perturbed, a dual
+                                   infeasible basis is repaired by shifting the
+                                   wrong-signed nonbasic costs instead of phase 1 */
 } or_options;
 
 typedef struct or_result {

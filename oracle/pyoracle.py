@@ -22,7 +22,8 @@ class OrOptions(C.Structure):
                 ("strict_reference", C.c_int), ("seed", C.c_ulonglong),
                 ("gpu_control_flow", C.c_int), ("verbose", C.c_int), ("var_weight", C.c_void_p),
                 ("harris", C.c_int), ("block_lu", C.c_int), ("rt_rel_tol", C.c_double),
-                ("col_rel_tol", C.c_double), ("pivot_abs_tol", C.c_double)]
+                ("col_rel_tol", C.c_double), ("pivot_abs_tol", C.c_double),
+                ("shift_costs", C.c_int)]
 
 
 class OrResult(C.Structure):
