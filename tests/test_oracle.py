@@ -164,3 +164,18 @@ def test_oracle_block_factorisation(block_lu):
         r = po.solve_typed(L.typed(lp), block_lu=block_lu)
         assert r["status"] == "optimal"
         assert abs(r["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
+
+
+def test_oracle_stabilised_rules_reach_highs_optimum():
+    """The oracle's experimental stabilisation for large LPs (pivot tolerance
+    1e-2 in the ratio test, cost shifting instead of phase 1 once the costs are
+    perturbed, block-triangular LU) on a 3000 x 6000 LP of the large workload's
+    generator: HiGHS's optimum, with hardly any phase 1."""
+    from parallel_ds_b200 import _lib
+    lp = L.generate(_lib.GEN_PER_COL, 3000, 6000, per_col=8, seed=0)
+    r = po.solve_typed(L.typed(lp), block_lu=2, pivot_abs_tol=1e-2, shift_costs=1)
+    h = highs(lp)
+    assert r["status"] == "optimal"
+    assert abs(r["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
+    assert r["phase1_iterations"] < 100
+    assert r["min_pivot"] >= 1e-2 * 0.5
