@@ -646,12 +646,33 @@ def reference_arm(args):
     lps = [[G.typed(ref_gen(2000 + s * args.concurrency + c)) for c in range(per_step)]
            for s in range(K)]
     po.solve_typed(G.typed(G.plain_small(1000)))      # warm-up: load the library, fault in pages
+    large = args.workload == "plain_large"
+    # the large workload is timed like the GPU arm's line, over each LP's first
+    # iterations (a bounded sample: 300, the CPU port's dense LU grows with the bump)
+    cap = min(args.large_iters, 300) if large else None
+    solve = (lambda t: po.solve_typed(t, max_iterations=cap)) if large else po.solve_typed
     rs = []
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=per_step) as ex:
         for row in lps:
-            rs += list(ex.map(po.solve_typed, row))
+            rs += list(ex.map(solve, row))
     dt = time.perf_counter() - t0
+    if large:
+        its = sum(r["iterations"] for r in rs)
+        v = its / dt
+        return {
+            "metric": "iterations/s of the plain GPU dual simplex (eta file + sparse LU), first %d iterations"
+                      % args.large_iters,
+            "value": v, "unit": "iterations/s", "n_gpus": 0, "steps": K, "warmup": W, "ms_per_step": dt * 1e3 / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic: the GPU arm's seeded LPs",
+            "config": {"workload": WORKLOADS[args.workload]["desc"], "pricing": "dse",
+                       "step": f"{per_step} LPs, their first {cap} iterations, one per host thread"},
+            "cpu_baseline": {"value": v, "unit": "iterations/s", "cores": per_step, "kind": "port",
+                             "sample": f"{len(rs)} LPs, first {cap} iterations each, {its} iterations, {dt:.1f} s"},
+            "e2e": {"value": v, "unit": "iterations/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "statuses": sorted({r["status"] for r in rs}),
+        }
     solved = sum(1 for r in rs if r["status"] == "optimal")
     v = solved / dt
     return {
