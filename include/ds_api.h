@@ -328,7 +328,8 @@ int ds_kernel_ratio_test(int n, int N, const int* nonbasis, const double* alpha,
  * may be NULL.  The call copies its result back and synchronises its stream
  * before it returns, so it makes CUDA calls of its own: it must not be made
  * from inside a host function queued on a stream (cudaLaunchHostFunc), where
- * CUDA calls are not allowed. */
+ * CUDA calls are not allowed, nor on a stream that is being captured into a
+ * CUDA graph (the synchronisation ends the capture with an error). */
 #define DS_NOALLOC_MAX_SLOTS 65536
 int ds_kernel_ratio_test_noalloc(int n, int N, const int* nonbasis, const double* alpha,
                                  double delta, int is_lower, const double* x, const double* d,
