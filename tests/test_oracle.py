@@ -179,3 +179,18 @@ def test_oracle_stabilised_rules_reach_highs_optimum():
     assert abs(r["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
     assert r["phase1_iterations"] < 100
     assert r["min_pivot"] >= 1e-2 * 0.5
+
+
+def test_oracle_column_relative_pivot_refusal():
+    """The oracle's experimental refusal of a pivot that is small against its own
+    FTRAN column (|alpha_q[p]| < col_rel_tol * max|alpha_q|): the row is blocked
+    for a while, the basis refactorised, and the solve still ends at HiGHS's
+    optimum, with every pivot taken above the bar."""
+    from parallel_ds_b200 import _lib
+    lp = L.generate(_lib.GEN_PER_COL, 600, 1200, per_col=8, seed=2)
+    r = po.solve_typed(L.typed(lp), col_rel_tol=1e-3)
+    h = highs(lp)
+    assert r["status"] == "optimal"
+    assert abs(r["objective"] - h.fun) <= 1e-9 * max(1.0, abs(h.fun))
+    assert r["refused_pivots"] > 0
+    assert r["min_pivot_rel"] >= 1e-3
